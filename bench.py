@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Throughput of the mCDFCI iteration on one B200 (N ranks = N replicas).
+
+Workload: the synthetic 24-orbital, 6 alpha + 6 beta electron Hamiltonian
+(~1.8e10 determinants, mcdfci_b200.synth "n24_6a6b", seed 0) with
+num_of_coordinate = estimate = 32, max_memory = 64 GB, z_threshold = 1e-9,
+FP64.  A step is one iteration of the hot path: pick 32 coordinates, generate
+their 32 Hamiltonian columns (16,471 entries each), solve the 33x33 subspace
+eigenproblem, apply x += dx and z += H_col * dx in the hash wavefunction.
+
+  value        coordinate updates/s over all ranks (32 per step per rank),
+               from CUDA events on the solver's stream, max over ranks
+  e2e          the same metric through the C ABI a user calls
+               (mcd_create_from_fcidump from host data + mcd_solve + read of
+               the result), wall clock, host<->device copies inside
+  roofline     column kernel: 40 algorithmic bytes per column entry (16-byte
+               key probe, 8-byte x read, 8-byte z read, 8-byte z write) over
+               its average device time, against the measured HBM copy peak
+  cpu_baseline the reference cdfci_omp, compiled from its sources, on a
+               bounded sample of the same workload on this host's cores
+
+Multi-GPU: the iteration does not shard (a sequential block Gauss-Southwell
+chain), so --gpus N runs N independent replicas with no collective on the
+data path ("weak" scaling).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "coord updates/s"
+UNIT = "coordinate_updates/s"
+WORKLOAD = "n24_6a6b"
+BYTES_PER_ENTRY = 40
+REF_EXE = os.path.join(HERE, "oracle", "_ref", "cdfci_omp")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=400)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--k", type=int, default=32)
+    ap.add_argument("--m", type=int, default=32)
+    ap.add_argument("--max-memory", type=float, default=64.0)
+    ap.add_argument("--z-threshold", type=float, default=1e-9)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=600, help="reference iterations timed for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def config(args):
+    return {
+        "workload": f"{WORKLOAD}: norb=24, 6a/6b (~1.8e10 dets), synthetic seed {args.seed}",
+        "num_of_coordinate": args.k,
+        "estimate": args.m,
+        "max_memory_gb": args.max_memory,
+        "z_threshold": args.z_threshold,
+        "step": "one mCDFCI iteration",
+        "l2": "inputs larger than L2: the hash wavefunction is 68.7 GB (2^31 slots x 32 B) vs 126 MB L2",
+        "parallelism": "replicas",
+    }
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+             "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per column-kernel launch from the committed ncu summary."""
+    p = os.path.join(HERE, "profiles", "column_kernel_n24_6a6b.md")
+    try:
+        txt = open(p).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+def write_workload(d, seed):
+    from mcdfci_b200 import synth
+
+    path = os.path.join(d, WORKLOAD + ".fcidump")
+    synth.write_fcidump(path, WORKLOAD, seed=seed)
+    return path
+
+
+# ---------------------------------------------------------------------------
+# The reference solver, built from its sources (oracle/Makefile).
+
+def run_reference(fcidump, k, m, zt, warmup, steps, max_memory, threads):
+    """Runs cdfci_omp for warmup+steps iterations; returns (updates/s, k_eff,
+    seconds) measured from its own cumulative timer between the report at
+    `warmup` and the one at `warmup+steps`."""
+    r = math.gcd(warmup, steps) if warmup > 0 else steps
+    with tempfile.TemporaryDirectory() as d:
+        deck = os.path.join(d, "input.json")
+        with open(deck, "w") as f:
+            json.dump({"hamiltonian": {"fcidump_path": fcidump, "threshold": 0.0},
+                       "solver": {"cdfci": {"num_iterations": warmup + steps, "report_interval": r,
+                                            "z_threshold": zt, "z_threshold_search": False,
+                                            "max_memory": max_memory, "coordinate_pick": "gcd_grad",
+                                            "coordinate_update": "eig", "num_of_coordinate": k,
+                                            "estimate": m}}}, f)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+        res = subprocess.run([REF_EXE, deck], capture_output=True, text=True, env=env, timeout=1800)
+    if res.returncode != 0:
+        raise RuntimeError("reference failed: " + (res.stderr or res.stdout)[-500:])
+    k_eff = k
+    m_warn = re.search(r"Not enough processes\. Set k = (\d+)", res.stdout)
+    if m_warn:
+        k_eff = int(m_warn.group(1))
+    times = {}
+    for line in res.stdout.splitlines():
+        p = line.split()
+        if len(p) >= 9 and re.match(r"^\d+$", p[0]) and re.match(r"^-?\d+\.\d+$", p[1]):
+            times[int(p[0])] = float(p[7])
+    t0 = times.get(warmup, 0.0)
+    t1 = times[warmup + steps]
+    dt = t1 - t0
+    return k_eff * steps / dt, k_eff, dt
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_EXE):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cdfci_omp not built (needs the reference sources)"}))
+        return 0
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        path = write_workload(d, args.seed)
+        # The reference allocates its whole table in host RAM up front; a
+        # smaller max_memory keeps the run within this host's memory and
+        # does not change the per-iteration work until the table fills.
+        mem = min(args.max_memory, 4.0)
+        rate, k_eff, dt = run_reference(path, args.k, args.m, args.z_threshold, args.warmup, args.steps, mem, threads)
+    sample = (f"{args.steps} iterations after {args.warmup} warm-up, k={k_eff} (capped at the core count), "
+              f"max_memory {mem} GB, OMP_NUM_THREADS={threads}, OPENBLAS_NUM_THREADS=1")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (mcdfci_b200.synth)", "config": config(args),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+
+def b200_arm(args, rank, world, local_rank):
+    import torch
+
+    import mcdfci_b200 as mc
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    tmp = tempfile.mkdtemp(prefix="mcd_bench_")
+    try:
+        path = write_workload(tmp, args.seed)
+        fc = mc.Fcidump(path)
+        solver = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
+                          z_threshold=args.z_threshold, threshold=0.0, device=local_rank)
+        solver.reset()
+        solver.run_iterations(args.warmup)
+        r0 = solver.report()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local_rank)
+        sampler.start()
+        time.sleep(0.3)
+        t = solver.run_iterations_timed(args.steps)
+        torch.cuda.synchronize()
+        sampler.stop()
+        if dist:
+            dist.barrier()
+        r1 = solver.report()
+        clocks = sampler.summary()
+        total_s = t["total_ms"] / 1000.0
+        entries = r1["emitted_total"] - r0["emitted_total"]
+        updates = args.k * args.steps
+        col_ms_avg = t["column_ms"] / args.steps
+        if dist:
+            tt = torch.tensor([total_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total_max = float(tt.item())
+        else:
+            total_max = total_s
+        value = world * updates / total_max
+        solver.close()
+
+        peak, peak_kind = hbm_peak()
+        achieved = (entries / args.steps) * BYTES_PER_ENTRY / (col_ms_avg / 1000.0) / 1e9
+        traffic = ncu_traffic()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "peak_source": peak_kind,
+                    "kernel": "column_kernel", "entries_per_launch": entries / args.steps,
+                    "algorithmic_bytes_per_entry": BYTES_PER_ENTRY, "avg_launch_ms": col_ms_avg,
+                    "leader_ms_per_step": t["leader_ms"] / args.steps}
+
+        e2e = None
+        if not args.no_e2e:
+            e2e = e2e_run(mc, fc, args, local_rank)
+            if dist:
+                tt = torch.tensor([e2e["seconds"]], dtype=torch.float64, device="cuda")
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                e2e["value"] = world * args.k * e2e["iterations"] / float(tt.item())
+
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_EXE):
+            threads = os.cpu_count() or 1
+            n = args.cpu_sample
+            w = max(100, n // 5)
+            try:
+                rate, k_eff, dt = run_reference(path, args.k, args.m, args.z_threshold, w, n, 4.0, threads)
+                cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"{n} iterations after {w} warm-up of the same workload, k={k_eff} "
+                                 f"(the reference caps k at the core count), max_memory 4 GB, "
+                                 f"OMP_NUM_THREADS={threads}, {dt:.1f} s"}
+            except Exception as e:  # reported, not fatal
+                cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": f"failed: {e}"}
+
+        if rank == 0:
+            out = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * total_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (mcdfci_b200.synth)",
+                "config": config(args),
+                "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")} if e2e else None,
+                "gpu_launches": 2 * args.steps,
+                "roofline": roofline,
+                "cpu_baseline": cpu,
+                "clocks": clocks,
+                "energy": r1["energy"],
+                "z_size": r1["z_size"],
+                "e2e_detail": e2e,
+            }
+            print(json.dumps(out))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def e2e_run(mc, fc, args, local_rank):
+    """create (host tables -> device) + solve (reports read back) + result."""
+    import ctypes
+
+    iters = args.steps
+    interval = max(1, iters // 10)
+    t0 = time.perf_counter()
+    s = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
+                 z_threshold=args.z_threshold, threshold=0.0, device=local_rank, num_iterations=iters,
+                 report_interval=interval)
+    s.solve()
+    energy = s.result_energy
+    s.close()
+    dt = time.perf_counter() - t0
+    n = fc.norb
+    nsp = n // 2
+    table_bytes = 8 * (n + n * n + 2 * nsp * nsp + 2 * nsp * nsp * n + 2 * nsp + 2 * (nsp * (nsp - 1) // 2) ** 2 + nsp ** 4)
+    state_bytes = 16 * 1024
+    h2d = table_bytes + state_bytes
+    d2h = (iters // interval) * (state_bytes + 8)
+    return {"value": args.k * iters / dt, "unit": UNIT, "h2d_bytes_per_step": h2d / iters,
+            "d2h_bytes_per_step": d2h / iters, "seconds": dt, "iterations": iters, "energy": energy,
+            "what": "mcd_create_from_fcidump (Hamiltonian tables host->device, 64 GB table init) + mcd_solve "
+                    f"({iters} iterations, a report read back every {interval}) + mcd_result"}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return b200_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

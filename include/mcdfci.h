@@ -1,0 +1,189 @@
+/*
+ * mcdfci_b200 C ABI: multi-coordinate-descent FCI (mCDFCI) on one B200.
+ *
+ * Drop-in for the solver path of ninotreve/mcdfci's cdfci_omp.  The reference
+ * has no FFI; its boundary is run_cdfci<N>(Option&, Fcidump&) -> double
+ * (src/run_wrapper.h:124-173) over the C++ interfaces Hamiltonian<N>
+ * (src/hamiltonian.h:25-54), WaveFunction<N> (src/wavefunction.h:163-221),
+ * CoordinatePick<N> / CoordinateUpdate<N> (src/solver.h:94-101,230-250) and
+ * Solver / CDFCI<N> (src/solver.h:613-893).  The entry points below replace
+ * that boundary with plain pointers and sizes; no C++ exception and no CUDA
+ * or torch type crosses it.  Every function returns an MCD_* status; the text
+ * of the last error is available from mcd_last_error().
+ *
+ * Determinants cross the ABI as (alpha, beta) pairs of uint64 occupation
+ * strings: bit p of alpha is spatial orbital p with spin alpha.  The
+ * reference's layout interleaves them (bit 2p alpha, bit 2p+1 beta,
+ * src/input.h:242-243).
+ *
+ * All arithmetic is FP64; the solver scalars xx, scale and xz (__float128 in
+ * the reference) are double-double and cross the ABI as (hi, lo) pairs.
+ */
+#ifndef MCDFCI_H
+#define MCDFCI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MCD_OK 0
+/* z_threshold_search asks for a restart with a doubled z_threshold; the
+ * reference's CDFCI<N>::solve returns -1 (src/solver.h:803-808). */
+#define MCD_RESTART (-1)
+#define MCD_ERR_INVALID 1      /* bad input or option (std::invalid_argument in the reference) */
+#define MCD_ERR_OVERFLOW 2     /* "The hash table is full..." (std::overflow_error, src/solver.h:813-817) */
+#define MCD_ERR_EIG 3          /* subspace eigenproblem failed (the reference exits, src/solver.h:447-450) */
+#define MCD_ERR_CUDA 4         /* CUDA runtime error, or no usable GPU */
+#define MCD_ERR_UNSUPPORTED 5  /* outside this build's limits (norb > 64, k or estimate > 128, ...) */
+#define MCD_ERR_NO_CANDIDATES 6 /* the candidate list became empty */
+#define MCD_STOPPED 7          /* the report callback asked to stop */
+
+/* coordinate_pick / coordinate_update values (src/run_wrapper.h:136-156). */
+#define MCD_PICK_GCD_GRAD 0
+#define MCD_UPDATE_EIG 1
+#define MCD_UPDATE_LS 2 /* accepted by the reference but not implemented here: MCD_ERR_UNSUPPORTED */
+
+typedef struct mcd_solver mcd_solver;   /* opaque: one solver bound to one GPU */
+typedef struct mcd_fcidump mcd_fcidump; /* opaque: a parsed FCIDUMP (host memory) */
+
+/* Integrals in spin-orbital form, as the reference's Fcidump holds them
+ * (src/input.h:57-86). */
+typedef struct mcd_problem {
+  int32_t norb;   /* spin-orbitals: 2 x NORB for RHF, NORB for UHF; even, <= 128 */
+  int32_t nelec;
+  int32_t ms2;
+  int32_t uhf;
+  double core_energy;
+  const double* h1;             /* [norb*norb] <i|h|a> */
+  const double* g2;             /* [norb^4] <ij|ab> at ((i*norb+j)*norb+a)*norb+b; used for i <= j, 0 = absent */
+  const double* orbital_energy; /* [norb] or NULL (then the Hartree-Fock guess assumes index order) */
+} mcd_problem;
+
+/* The solver:cdfci and hamiltonian options of the input deck, with the
+ * reference's defaults (src/run_wrapper.h:64-80) set by mcd_options_default. */
+typedef struct mcd_options {
+  int64_t num_iterations;      /* 10 */
+  int64_t report_interval;     /* 1 */
+  int32_t num_of_coordinate;   /* k, 1 */
+  int32_t estimate;            /* m, 100 */
+  double z_threshold;          /* 0 */
+  int32_t z_threshold_search;  /* 0 */
+  double max_memory;           /* GB for the wavefunction; required > 0 */
+  double threshold;            /* hamiltonian:threshold, 1e-13 */
+  const int32_t* ref_det_occ;  /* NULL, or spin-orbital indices of the reference determinant */
+  int32_t n_ref_det_occ;
+  int32_t coordinate_pick;     /* MCD_PICK_GCD_GRAD */
+  int32_t coordinate_update;   /* MCD_UPDATE_EIG (the reference's default, "ls", is unsupported) */
+  int32_t cluster;             /* CTAs per Hamiltonian column, 1..16; 0 = chosen from the column length */
+  int32_t verbose;             /* 1: print the reference's report table to stdout */
+  void* stream;                /* cudaStream_t to run on; NULL = a stream owned by the solver */
+  int32_t device;              /* CUDA device ordinal; -1 = the current device */
+} mcd_options;
+
+/* One line of the reference's report table (src/solver.h:761-798). */
+typedef struct mcd_report {
+  int64_t iteration;
+  double energy;        /* xz / xx */
+  double dx_max;        /* |dx|_max of the last iteration */
+  uint64_t x_size;      /* |x|_0 */
+  uint64_t z_size;      /* |z|_0 */
+  uint64_t cols_size;   /* |H[I]|_0: column entries of the last iteration */
+  uint64_t updates;     /* upds: z updates of the last iteration */
+  double time_s;        /* wall time since the start of the solve */
+  double scale;
+  double max_residual;  /* max ||B v - lambda v|| of the subspace eigenproblems */
+  double z_threshold;
+  uint64_t emitted_total; /* column entries processed since the last reset */
+  uint64_t updates_total; /* z updates since the last reset */
+  uint64_t occupied;      /* occupied hash slots */
+  int32_t last_k;         /* determinants picked in the last iteration */
+} mcd_report;
+
+/* Called after every report_interval iterations; return nonzero to stop. */
+typedef int (*mcd_report_cb)(const mcd_report* report, void* user);
+
+/* ---- Input ------------------------------------------------------------- */
+
+/* Fcidump::Fcidump(path) (src/input.h:88-152). */
+int mcd_fcidump_read(const char* path, mcd_fcidump** out);
+/* A view of the parsed integrals; valid until mcd_fcidump_free.
+ * orbital_energy is NULL unless the FCIDUMP lists an energy for every orbital. */
+int mcd_fcidump_problem(const mcd_fcidump* f, mcd_problem* view);
+void mcd_fcidump_free(mcd_fcidump* f);
+
+/* Defaults of read_input (src/run_wrapper.h:61-80). */
+void mcd_options_default(mcd_options* o);
+
+/* ---- Solver ------------------------------------------------------------ */
+
+/* HamiltonianMolecule<N>(fci, threshold) + CDFCI<N>(option) + the table
+ * sizing of run_cdfci_wrapper (src/run_wrapper.h:203-213): builds the
+ * Hamiltonian tables on the GPU and allocates the hash wavefunction. */
+int mcd_create(const mcd_problem* problem, const mcd_options* options, mcd_solver** out);
+/* The same, from a parsed FCIDUMP, keeping its orbital energies as read
+ * (a partial list included), as run_cdfci_wrapper does (src/run_wrapper.h:175-241). */
+int mcd_create_from_fcidump(const mcd_fcidump* f, const mcd_options* options, mcd_solver** out);
+void mcd_destroy(mcd_solver* s);
+
+/* CDFCI<N>::solve(h, pick, update, k, m) (src/solver.h:831-893): initial
+ * state, num_iterations iterations with a report every report_interval,
+ * restarts with a doubled z_threshold under z_threshold_search.  Returns
+ * MCD_OK or an error status. */
+int mcd_solve(mcd_solver* s, mcd_report_cb cb, void* user);
+
+/* Lower-level control (bench and tests).  mcd_reset puts the wavefunction in
+ * the initial state (x = e_ref, z = H[:, ref], src/solver.h:862-873);
+ * mcd_run_iterations enqueues n iterations on the solver's stream without
+ * waiting; mcd_get_report waits and reads the state. */
+int mcd_reset(mcd_solver* s);
+int mcd_run_iterations(mcd_solver* s, int64_t n);
+/* n iterations with a CUDA event recorded on the solver's stream between
+ * every two kernels; waits and returns the summed device time of the leader
+ * kernels, of the column kernels, and the total, in milliseconds. */
+int mcd_run_iterations_timed(mcd_solver* s, int64_t n, double* leader_ms, double* column_ms, double* total_ms);
+int mcd_get_report(mcd_solver* s, mcd_report* r);
+/* Solver::result_energy (src/solver.h:613-619) of the last solve. */
+int mcd_result(const mcd_solver* s, double* energy);
+/* The cudaStream_t the solver runs on. */
+int mcd_stream(const mcd_solver* s, void** stream);
+/* Solver-side scalars: xx, scale, xz as (hi, lo) pairs; iteration count. */
+int mcd_scalars(mcd_solver* s, double xx[2], double scale[2], double xz[2], int64_t* iteration);
+
+/* Text of the last error on this thread. */
+const char* mcd_last_error(void);
+
+/* The whole cdfci_omp main (src/main.cpp:19-36): read the JSON input deck,
+ * the FCIDUMP it names, print the header and the report table, solve.
+ * Returns 0 on success and 1 on error, as main does. */
+int mcd_run_json(const char* input_json_path);
+
+/* ---- Parity / debug ---------------------------------------------------- */
+
+/* HamiltonianMolecule::get_column (src/hamiltonian.h:412-424) of one
+ * determinant: up to `cap` (alpha, beta, value) entries, in this build's
+ * enumeration order.  *n_out receives the total count. */
+int mcd_debug_column(mcd_solver* s, uint64_t alpha, uint64_t beta, uint64_t* alpha_out, uint64_t* beta_out,
+                     double* value_out, int64_t cap, int64_t* n_out);
+/* CDFCI::get_hamiltonian_submatrix (src/solver.h:637-670): H[i*k+j] =
+ * get_off_diagonal(det_i, det_j) for i != j, get_diagonal on the diagonal. */
+int mcd_debug_hsub(mcd_solver* s, const uint64_t* alpha, const uint64_t* beta, int32_t k, double* hsub);
+/* CoordinateUpdateEig::operator() (src/solver.h:333-609) on given inputs, on
+ * the current CUDA device: returns dx[k], the new xx and scale as (hi, lo),
+ * and the branch (1: (k+1)x(k+1) problem, 2: k x k first-iteration problem). */
+int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                  const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch);
+/* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
+ * sum over the table of x^2 and x*z (double-double), and the slot count. */
+int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
+/* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
+int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCDFCI_H */

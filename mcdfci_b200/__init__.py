@@ -1,0 +1,422 @@
+"""mcdfci_b200: multi-coordinate-descent FCI (mCDFCI) on one B200.
+
+Python binding of the C ABI in include/mcdfci.h (libmcdfci.so, built in-tree
+by ``python -c "import __graft_entry__; __graft_entry__.build()"`` or
+``make -C mcdfci_b200/csrc``).  The classes mirror the reference's interfaces
+(ninotreve/mcdfci src/): ``Fcidump`` (input.h), ``Determinant``
+(determinant.h), ``CDFCI`` (the Solver of solver.h, owning the Hamiltonian
+tables and the hash WaveFunction on the GPU).
+
+There is no CPU fallback: every compute call goes through libmcdfci.so and the
+sm_100a kernels; importing the solver without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Callable, Iterable, List, Optional, Sequence, Tuple
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmcdfci.so")
+CLI_PATH = os.path.join(_HERE, "mcdfci")
+
+MCD_OK = 0
+MCD_RESTART = -1
+MCD_ERR_INVALID = 1
+MCD_ERR_OVERFLOW = 2
+MCD_ERR_EIG = 3
+MCD_ERR_CUDA = 4
+MCD_ERR_UNSUPPORTED = 5
+MCD_ERR_NO_CANDIDATES = 6
+MCD_STOPPED = 7
+MCD_PICK_GCD_GRAD = 0
+MCD_UPDATE_EIG = 1
+MCD_UPDATE_LS = 2
+
+# Every symbol include/mcdfci.h declares.
+EXPORTED_SYMBOLS = (
+    "mcd_fcidump_read", "mcd_fcidump_problem", "mcd_fcidump_free", "mcd_options_default",
+    "mcd_create", "mcd_create_from_fcidump", "mcd_destroy", "mcd_solve", "mcd_reset",
+    "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
+    "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
+    "mcd_debug_table_sums", "mcd_debug_picked",
+)
+
+
+class McdError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+class mcd_problem(ctypes.Structure):
+    _fields_ = [
+        ("norb", ctypes.c_int32), ("nelec", ctypes.c_int32), ("ms2", ctypes.c_int32), ("uhf", ctypes.c_int32),
+        ("core_energy", ctypes.c_double),
+        ("h1", ctypes.POINTER(ctypes.c_double)), ("g2", ctypes.POINTER(ctypes.c_double)),
+        ("orbital_energy", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class mcd_options(ctypes.Structure):
+    _fields_ = [
+        ("num_iterations", ctypes.c_int64), ("report_interval", ctypes.c_int64),
+        ("num_of_coordinate", ctypes.c_int32), ("estimate", ctypes.c_int32),
+        ("z_threshold", ctypes.c_double), ("z_threshold_search", ctypes.c_int32),
+        ("max_memory", ctypes.c_double), ("threshold", ctypes.c_double),
+        ("ref_det_occ", ctypes.POINTER(ctypes.c_int32)), ("n_ref_det_occ", ctypes.c_int32),
+        ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
+        ("cluster", ctypes.c_int32), ("verbose", ctypes.c_int32),
+        ("stream", ctypes.c_void_p), ("device", ctypes.c_int32),
+    ]
+
+
+class mcd_report(ctypes.Structure):
+    _fields_ = [
+        ("iteration", ctypes.c_int64), ("energy", ctypes.c_double), ("dx_max", ctypes.c_double),
+        ("x_size", ctypes.c_uint64), ("z_size", ctypes.c_uint64), ("cols_size", ctypes.c_uint64),
+        ("updates", ctypes.c_uint64), ("time_s", ctypes.c_double), ("scale", ctypes.c_double),
+        ("max_residual", ctypes.c_double), ("z_threshold", ctypes.c_double),
+        ("emitted_total", ctypes.c_uint64), ("updates_total", ctypes.c_uint64), ("occupied", ctypes.c_uint64),
+        ("last_k", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+REPORT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(mcd_report), ctypes.c_void_p)
+
+_lib = None
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def library() -> ctypes.CDLL:
+    """Load libmcdfci.so.  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {os.path.join(_HERE, 'csrc')}`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.mcd_fcidump_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.mcd_fcidump_problem.argtypes = [vp, ctypes.POINTER(mcd_problem)]
+    L.mcd_fcidump_free.argtypes = [vp]
+    L.mcd_fcidump_free.restype = None
+    L.mcd_options_default.argtypes = [ctypes.POINTER(mcd_options)]
+    L.mcd_options_default.restype = None
+    L.mcd_create.argtypes = [ctypes.POINTER(mcd_problem), ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
+    L.mcd_create_from_fcidump.argtypes = [vp, ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
+    L.mcd_destroy.argtypes = [vp]
+    L.mcd_destroy.restype = None
+    L.mcd_solve.argtypes = [vp, REPORT_CB, vp]
+    L.mcd_reset.argtypes = [vp]
+    L.mcd_run_iterations.argtypes = [vp, ctypes.c_int64]
+    L.mcd_run_iterations_timed.argtypes = [vp, ctypes.c_int64, _dp, _dp, _dp]
+    L.mcd_get_report.argtypes = [vp, ctypes.POINTER(mcd_report)]
+    L.mcd_result.argtypes = [vp, _dp]
+    L.mcd_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.mcd_scalars.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.mcd_last_error.restype = ctypes.c_char_p
+    L.mcd_last_error.argtypes = []
+    L.mcd_run_json.argtypes = [ctypes.c_char_p]
+    L.mcd_debug_column.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, _u64p, _u64p, _dp, ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_int64)]
+    L.mcd_debug_hsub.argtypes = [vp, _u64p, _u64p, ctypes.c_int32, _dp]
+    L.mcd_debug_eig.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
+    L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> int:
+    if rc != MCD_OK:
+        raise McdError(rc, library().mcd_last_error().decode(errors="replace"))
+    return rc
+
+
+# ---------------------------------------------------------------------------
+
+class Determinant:
+    """A determinant as (alpha, beta) occupation strings (Determinant<N>,
+    src/determinant.h:24-123, stores the same bits interleaved)."""
+
+    __slots__ = ("alpha", "beta")
+
+    def __init__(self, alpha: int, beta: int):
+        self.alpha = int(alpha)
+        self.beta = int(beta)
+
+    @classmethod
+    def from_spin_orbitals(cls, occ: Iterable[int]) -> "Determinant":
+        a = b = 0
+        for so in occ:
+            if so & 1:
+                b |= 1 << (so >> 1)
+            else:
+                a |= 1 << (so >> 1)
+        return cls(a, b)
+
+    def spin_orbitals(self) -> List[int]:
+        out = []
+        p = 0
+        while (self.alpha >> p) or (self.beta >> p):
+            if (self.alpha >> p) & 1:
+                out.append(2 * p)
+            if (self.beta >> p) & 1:
+                out.append(2 * p + 1)
+            p += 1
+        return out
+
+    def interleaved(self, nw: int) -> List[int]:
+        """The reference's repr words."""
+        bits = 0
+        for so in self.spin_orbitals():
+            bits |= 1 << so
+        return [(bits >> (64 * t)) & 0xFFFFFFFFFFFFFFFF for t in range(nw)]
+
+    @classmethod
+    def from_interleaved(cls, words: Sequence[int]) -> "Determinant":
+        bits = 0
+        for t, w in enumerate(words):
+            bits |= int(w) << (64 * t)
+        occ = [i for i in range(bits.bit_length()) if (bits >> i) & 1]
+        return cls.from_spin_orbitals(occ)
+
+    def key(self) -> Tuple[int, int]:
+        return (self.alpha, self.beta)
+
+    def __eq__(self, other):
+        return isinstance(other, Determinant) and self.key() == other.key()
+
+    def __hash__(self):
+        return hash(self.key())
+
+    def __repr__(self):
+        return f"Determinant(alpha={self.alpha:#x}, beta={self.beta:#x})"
+
+
+class Fcidump:
+    """A parsed FCIDUMP (Fcidump, src/input.h:57-338), host memory."""
+
+    def __init__(self, path: str):
+        L = library()
+        h = ctypes.c_void_p()
+        _check(L.mcd_fcidump_read(path.encode(), ctypes.byref(h)))
+        self._h = h
+        self.problem = mcd_problem()
+        _check(L.mcd_fcidump_problem(self._h, ctypes.byref(self.problem)))
+        self.path = path
+
+    @property
+    def norb(self) -> int:
+        return self.problem.norb
+
+    @property
+    def nelec(self) -> int:
+        return self.problem.nelec
+
+    @property
+    def ms2(self) -> int:
+        return self.problem.ms2
+
+    @property
+    def core_energy(self) -> float:
+        return self.problem.core_energy
+
+    def arrays(self):
+        """(h1[norb, norb], g2[norb]*4) as numpy views of the parsed data."""
+        import numpy as np
+
+        n = self.norb
+        h1 = np.ctypeslib.as_array(self.problem.h1, shape=(n, n))
+        g2 = np.ctypeslib.as_array(self.problem.g2, shape=(n, n, n, n))
+        return h1, g2
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().mcd_fcidump_free(self._h)
+            self._h = None
+
+
+def make_options(**kw) -> mcd_options:
+    """mcd_options with the reference defaults, then keyword overrides
+    (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
+    z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
+    ("eig"|"ls"), cluster, verbose, stream, device)."""
+    o = mcd_options()
+    library().mcd_options_default(ctypes.byref(o))
+    occ = kw.pop("ref_det_occ", None)
+    upd = kw.pop("coordinate_update", None)
+    if upd is not None:
+        o.coordinate_update = {"eig": MCD_UPDATE_EIG, "ls": MCD_UPDATE_LS}[upd] if isinstance(upd, str) else int(upd)
+    for k, v in kw.items():
+        if k == "stream":
+            o.stream = ctypes.c_void_p(int(v) if v else 0)
+        elif k == "z_threshold_search":
+            o.z_threshold_search = int(bool(v))
+        else:
+            setattr(o, k, v)
+    if occ:
+        arr = (ctypes.c_int32 * len(occ))(*occ)
+        o.ref_det_occ = ctypes.cast(arr, ctypes.POINTER(ctypes.c_int32))
+        o.n_ref_det_occ = len(occ)
+        o._occ_keepalive = arr  # type: ignore[attr-defined]
+    return o
+
+
+class CDFCI:
+    """The mCDFCI solver on one GPU (CDFCI<N>, src/solver.h:621-920).
+
+    ``CDFCI(Fcidump(path), num_of_coordinate=8, estimate=8, max_memory=0.005,
+    num_iterations=20000, report_interval=1000)`` builds the Hamiltonian
+    tables and the hash wavefunction on the GPU; ``solve()`` runs the
+    reference's iteration and returns the energy.
+    """
+
+    def __init__(self, source, **options):
+        L = library()
+        self._opts = make_options(**options)
+        h = ctypes.c_void_p()
+        if isinstance(source, Fcidump):
+            self._fcidump = source
+            _check(L.mcd_create_from_fcidump(source._h, ctypes.byref(self._opts), ctypes.byref(h)))
+        elif isinstance(source, mcd_problem):
+            _check(L.mcd_create(ctypes.byref(source), ctypes.byref(self._opts), ctypes.byref(h)))
+        else:
+            self._fcidump = Fcidump(str(source))
+            _check(L.mcd_create_from_fcidump(self._fcidump._h, ctypes.byref(self._opts), ctypes.byref(h)))
+        self._h = h
+        self.reports: List[dict] = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().mcd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- solve ------------------------------------------------------------
+    def solve(self, callback: Optional[Callable[[dict], bool]] = None) -> float:
+        self.reports = []
+
+        def cb(rep, _user):
+            d = rep.contents.as_dict()
+            self.reports.append(d)
+            return 1 if (callback is not None and callback(d)) else 0
+
+        c = REPORT_CB(cb)
+        rc = library().mcd_solve(self._h, c, None)
+        if rc not in (MCD_OK, MCD_STOPPED):
+            _check(rc)
+        return self.result_energy
+
+    @property
+    def result_energy(self) -> float:
+        e = ctypes.c_double()
+        _check(library().mcd_result(self._h, ctypes.byref(e)))
+        return e.value
+
+    # -- lower-level control ---------------------------------------------
+    def reset(self):
+        _check(library().mcd_reset(self._h))
+
+    def run_iterations(self, n: int):
+        _check(library().mcd_run_iterations(self._h, int(n)))
+
+    def run_iterations_timed(self, n: int) -> dict:
+        """n iterations with per-kernel CUDA events; device times in ms."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(library().mcd_run_iterations_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b),
+                                                  ctypes.byref(c)))
+        return {"leader_ms": a.value, "column_ms": b.value, "total_ms": c.value}
+
+    def report(self) -> dict:
+        r = mcd_report()
+        _check(library().mcd_get_report(self._h, ctypes.byref(r)))
+        return r.as_dict()
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(library().mcd_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def scalars(self) -> dict:
+        xx, sc, xz = (ctypes.c_double * 2)(), (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+        it = ctypes.c_int64()
+        _check(library().mcd_scalars(self._h, xx, sc, xz, ctypes.byref(it)))
+        return {"xx": tuple(xx), "scale": tuple(sc), "xz": tuple(xz), "iteration": it.value}
+
+    # -- parity / debug ---------------------------------------------------
+    def column(self, det: Determinant):
+        import numpy as np
+
+        n = ctypes.c_int64()
+        _check(library().mcd_debug_column(self._h, det.alpha, det.beta, None, None, None, 0, ctypes.byref(n)))
+        cap = n.value
+        a = np.zeros(cap, dtype=np.uint64)
+        b = np.zeros(cap, dtype=np.uint64)
+        v = np.zeros(cap)
+        _check(library().mcd_debug_column(self._h, det.alpha, det.beta, a.ctypes.data_as(_u64p),
+                                          b.ctypes.data_as(_u64p), v.ctypes.data_as(_dp), cap, ctypes.byref(n)))
+        return a, b, v
+
+    def hsub(self, dets: Sequence[Determinant]):
+        import numpy as np
+
+        k = len(dets)
+        a = np.array([d.alpha for d in dets], dtype=np.uint64)
+        b = np.array([d.beta for d in dets], dtype=np.uint64)
+        h = np.zeros(k * k)
+        _check(library().mcd_debug_hsub(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p), k,
+                                        h.ctypes.data_as(_dp)))
+        return h.reshape(k, k)
+
+    def table_sums(self) -> dict:
+        xx, xz = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+        occ = ctypes.c_uint64()
+        _check(library().mcd_debug_table_sums(self._h, xx, xz, ctypes.byref(occ)))
+        return {"xx": tuple(xx), "xz": tuple(xz), "occupied": occ.value}
+
+    def picked(self):
+        import numpy as np
+
+        cap = 128
+        a = np.zeros(cap, dtype=np.uint64)
+        b = np.zeros(cap, dtype=np.uint64)
+        dx = np.zeros(cap)
+        k = ctypes.c_int32()
+        _check(library().mcd_debug_picked(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
+                                          dx.ctypes.data_as(_dp), cap, ctypes.byref(k)))
+        return a[: k.value], b[: k.value], dx[: k.value]
+
+
+def debug_eig(hsub, x, z, xx, xz):
+    """CoordinateUpdateEig on one subproblem (src/solver.h:333-609), on the GPU.
+    xx, xz are (hi, lo) pairs.  Returns (dx, new_xx, new_scale, branch)."""
+    import numpy as np
+
+    hsub = np.ascontiguousarray(hsub, dtype=np.float64)
+    k = hsub.shape[0]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    dx = np.zeros(k)
+    nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+    br = ctypes.c_int32()
+    xxa = (ctypes.c_double * 2)(*xx)
+    xza = (ctypes.c_double * 2)(*xz)
+    _check(library().mcd_debug_eig(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+                                   xxa, xza, dx.ctypes.data_as(_dp), nxx, nsc, ctypes.byref(br)))
+    return dx, tuple(nxx), tuple(nsc), br.value
+
+
+def run_json(path: str) -> int:
+    """The cdfci_omp main on an input deck; returns 0 or 1."""
+    return library().mcd_run_json(path.encode())

@@ -1,0 +1,554 @@
+#include "gpu_solver.h"
+
+#include "device_common.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+
+namespace mcd {
+
+// ---------------------------------------------------------------------------
+// Table kernels.
+
+__global__ void table_fill_kernel(Slot* slots, size_t n) {
+  const Slot e{kEmptyKey, kEmptyKey, 0.0, 0.0};
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    slots[i] = e;
+}
+
+__global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsigned long long* count) {
+  __shared__ dd sxx[32], sxz[32];
+  dd axx{0, 0}, axz{0, 0};
+  unsigned long long c = 0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Slot s = slots[i];
+    if (s.a == kEmptyKey && s.b == kEmptyKey) continue;
+    ++c;
+    axx = dd_add(axx, dd_two_prod(s.x, s.x));
+    axz = dd_add(axz, dd_two_prod(s.x, s.z));
+  }
+  axx = warp_sum_dd(axx);
+  axz = warp_sum_dd(axz);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sxx[warp] = axx;
+    sxz[warp] = axz;
+  }
+  atomicAdd(count, c);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dd t1{0, 0}, t2{0, 0};
+    for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) {
+      t1 = dd_add(t1, sxx[w]);
+      t2 = dd_add(t2, sxz[w]);
+    }
+    partial[2 * blockIdx.x] = t1;
+    partial[2 * blockIdx.x + 1] = t2;
+  }
+}
+
+cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s) {
+  table_fill_kernel<<<148 * 8, 256, 0, s>>>(slots, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_table_sums(const Slot* slots, size_t n, dd* partial, unsigned long long* count, int nblocks,
+                              cudaStream_t s) {
+  table_sums_kernel<<<nblocks, 256, 0, s>>>(slots, n, partial, count);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <typename T>
+T* device_alloc(size_t count, const char* what) {
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess)
+    throw McdError(MCD_ERR_CUDA, std::string("cudaMalloc(") + what + ", " + std::to_string(count * sizeof(T)) +
+                                     " bytes): " + cudaGetErrorString(e));
+  return static_cast<T*>(p);
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+void GpuSolver::check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw McdError(MCD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
+  // Option validation (read_input, src/run_wrapper.h:89-119, and this build's limits).
+  if (opt_.coordinate_pick != MCD_PICK_GCD_GRAD)
+    throw McdError(MCD_ERR_INVALID, "the coordinate pick method is not implemented.");
+  if (opt_.coordinate_update == MCD_UPDATE_LS)
+    throw McdError(MCD_ERR_UNSUPPORTED,
+                   "coordinate_update \"ls\" is not implemented on the GPU; use \"eig\".");
+  if (opt_.coordinate_update != MCD_UPDATE_EIG)
+    throw McdError(MCD_ERR_INVALID, "the coordinate update method is not implemented.");
+  if (!(opt_.max_memory > 0.0))
+    throw McdError(MCD_ERR_INVALID,
+                   "solver:cdfci:max_memory is invalid. It is the maximum memory (GB) allowed for the "
+                   "wavefunction. Please set a positive number.");
+  if (opt_.report_interval < 1) throw McdError(MCD_ERR_INVALID, "solver:cdfci:report_interval must be >= 1.");
+  if (opt_.num_iterations < 0) throw McdError(MCD_ERR_INVALID, "solver:cdfci:num_iterations must be >= 0.");
+  if (opt_.z_threshold_search && opt_.report_interval < 1000)
+    throw McdError(MCD_ERR_INVALID, "Please set report_interval >= 1000 when z_threshold_search = true.");
+  if (opt_.k < 1 || opt_.k > kMaxK)
+    throw McdError(MCD_ERR_UNSUPPORTED, "num_of_coordinate must be in 1.." + std::to_string(kMaxK) + ".");
+  if (opt_.m < 1 || opt_.m > kMaxM)
+    throw McdError(MCD_ERR_UNSUPPORTED, "estimate must be in 1.." + std::to_string(kMaxM) + ".");
+  if (opt_.cluster < 0 || opt_.cluster > 16) throw McdError(MCD_ERR_INVALID, "cluster must be in 0..16.");
+  zt_ = opt_.z_threshold;
+  if (opt_.z_threshold_search && zt_ < 1e-10) zt_ = 1e-10;
+
+  try {
+    ham_ = build_hamiltonian(fci, opt_.threshold);
+    std::string warning;
+    if (opt_.ref_det_occ.empty()) {
+      ref_ = hartree_fock(fci, &warning);
+      if (!warning.empty() && opt_.verbose) std::cout << warning << std::endl << std::endl;
+    } else {
+      ref_ = ref_det_from_occ(fci, opt_.ref_det_occ);
+    }
+  } catch (const std::invalid_argument& e) {
+    throw McdError(MCD_ERR_INVALID, e.what());
+  }
+  ref_diag_ = diagonal_element(ham_, ref_);
+  na_ = __builtin_popcountll(ref_.a);
+  nb_ = __builtin_popcountll(ref_.b);
+  entries_ = column_entries(ham_.norb, na_, nb_);
+  if (entries_ < 0) throw McdError(MCD_ERR_UNSUPPORTED, "a Hamiltonian column has more than 2^31 entries.");
+  n_words_ = 1 + (fci.norb - 1) / 64;
+  if (opt_.cluster > 0) {
+    cluster_ = opt_.cluster;
+  } else {
+    cluster_ = std::max(1, std::min(16, (entries_ + 1023) / 1024));
+  }
+
+  // Table sizing as run_cdfci_wrapper (src/run_wrapper.h:203-213): the
+  // largest power of two of determinants whose reference footprint
+  // (8*N + 16 bytes) stays below max_memory; max_wavefunction_size is 0.79 of it.
+  const double bytes_per_det = static_cast<double>(n_words_ * 8 + 16);
+  size_t pow2 = 8;
+  while (static_cast<double>(pow2) * bytes_per_det < opt_.max_memory * 1073741824.0) pow2 *= 2;
+  pow2 /= 2;
+  capacity_ = pow2;
+  max_size_ = static_cast<unsigned long long>(0.79 * static_cast<double>(pow2));
+
+  // Device.
+  if (opt_.device >= 0) check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  check(cudaGetDevice(&device_), "cudaGetDevice");
+  if (opt_.stream) {
+    stream_ = opt_.stream;
+  } else {
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    own_stream_ = true;
+  }
+
+  try {
+    // Hamiltonian tables in one allocation.
+    const size_t n_hd = ham_.hdiag.size(), n_d2 = ham_.d2.size(), n_sh = ham_.sh.size(), n_st = ham_.st.size(),
+                 n_sp = ham_.spres.size(), n_vss = ham_.vss.size(), n_wab = ham_.wab.size();
+    size_t off = 0;
+    const size_t o_hd = off;
+    off = align_up(off + n_hd * 8, 256);
+    const size_t o_d2 = off;
+    off = align_up(off + n_d2 * 8, 256);
+    const size_t o_sh = off;
+    off = align_up(off + n_sh * 8, 256);
+    const size_t o_st = off;
+    off = align_up(off + n_st * 8, 256);
+    const size_t o_sp = off;
+    off = align_up(off + n_sp * 8, 256);
+    const size_t o_vss = off;
+    off = align_up(off + std::max<size_t>(n_vss, 1) * 8, 256);
+    const size_t o_wab = off;
+    off = align_up(off + n_wab * 8, 256);
+    d_tables_ = device_alloc<unsigned char>(off, "hamiltonian tables");
+    unsigned char* base = static_cast<unsigned char*>(d_tables_);
+    auto up = [&](size_t o, const void* src, size_t bytes) {
+      if (bytes) check(cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, stream_), "upload tables");
+    };
+    up(o_hd, ham_.hdiag.data(), n_hd * 8);
+    up(o_d2, ham_.d2.data(), n_d2 * 8);
+    up(o_sh, ham_.sh.data(), n_sh * 8);
+    up(o_st, ham_.st.data(), n_st * 8);
+    up(o_sp, ham_.spres.data(), n_sp * 8);
+    up(o_vss, ham_.vss.data(), n_vss * 8);
+    up(o_wab, ham_.wab.data(), n_wab * 8);
+    hd_.norb = ham_.norb;
+    hd_.nso = ham_.nso;
+    hd_.npair = ham_.npair;
+    hd_.ecore = ham_.ecore;
+    hd_.hdiag = reinterpret_cast<const double*>(base + o_hd);
+    hd_.d2 = reinterpret_cast<const double*>(base + o_d2);
+    hd_.sh = reinterpret_cast<const double*>(base + o_sh);
+    hd_.st = reinterpret_cast<const double*>(base + o_st);
+    hd_.spres = reinterpret_cast<const uint64_t*>(base + o_sp);
+    hd_.vss = reinterpret_cast<const double*>(base + o_vss);
+    hd_.wab = reinterpret_cast<const double*>(base + o_wab);
+
+    d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
+    d_state_ = device_alloc<IterState>(1, "iteration state");
+    d_cand_score_ = device_alloc<double>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
+    d_cand_slot_ = device_alloc<long long>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
+    d_hsub_ = device_alloc<double>(static_cast<size_t>(kMaxK) * kMaxK, "H_sub");
+    d_err_ = device_alloc<unsigned>(1, "error word");
+    d_occ_ = device_alloc<unsigned long long>(1, "occupancy");
+  } catch (...) {
+    release();
+    throw;
+  }
+
+  td_.slots = d_slots_;
+  td_.mask = capacity_ - 1;
+  td_.max_probe = static_cast<int>(std::min<size_t>(capacity_, 1u << 14));
+  td_.err = d_err_;
+  td_.n_occupied = d_occ_;
+
+  cl_.ham = hd_;
+  cl_.tab = td_;
+  cl_.st = d_state_;
+  cl_.cand_score = d_cand_score_;
+  cl_.cand_slot = d_cand_slot_;
+  cl_.m = opt_.m;
+  cl_.cap_w = ((opt_.m + 31) / 32) * 32 + 32;
+  cl_.cluster = cluster_;
+  cl_.k_grid = opt_.k;
+  cl_.na = na_;
+  cl_.nb = nb_;
+
+  ll_.ham = hd_;
+  ll_.tab = td_;
+  ll_.st = d_state_;
+  ll_.cand_score = d_cand_score_;
+  ll_.cand_slot = d_cand_slot_;
+  ll_.hsub_out = d_hsub_;
+  ll_.m = opt_.m;
+  ll_.k_req = opt_.k;
+  check(cudaStreamSynchronize(stream_), "table upload");
+}
+
+GpuSolver::~GpuSolver() { release(); }
+
+void GpuSolver::release() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  if (stream_) cudaStreamSynchronize(stream_);
+  cudaFree(d_tables_);
+  cudaFree(d_slots_);
+  cudaFree(d_state_);
+  cudaFree(d_cand_score_);
+  cudaFree(d_cand_slot_);
+  cudaFree(d_hsub_);
+  cudaFree(d_err_);
+  cudaFree(d_occ_);
+  d_tables_ = nullptr;
+  d_slots_ = nullptr;
+  d_state_ = nullptr;
+  d_cand_score_ = nullptr;
+  d_cand_slot_ = nullptr;
+  d_hsub_ = nullptr;
+  d_err_ = nullptr;
+  d_occ_ = nullptr;
+  if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+  stream_ = nullptr;
+  own_stream_ = false;
+}
+
+void GpuSolver::reset() {
+  check(launch_table_fill(d_slots_, capacity_, stream_), "table fill");
+  check(cudaMemsetAsync(d_err_, 0, sizeof(unsigned), stream_), "memset");
+  check(cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_), "memset");
+  std::memset(&h_state_, 0, sizeof(h_state_));
+  h_state_.zt = zt_;
+  h_state_.n_words = n_words_;
+  h_state_.k_req = opt_.k;
+  h_state_.m = opt_.m;
+  h_state_.occupancy_limit = static_cast<unsigned long long>(0.79 * static_cast<double>(max_size_));
+  check(cudaMemcpyAsync(d_state_, &h_state_, sizeof(IterState), cudaMemcpyHostToDevice, stream_), "state upload");
+  check(launch_init(ll_, ref_, ref_diag_, stream_), "init");
+  check(launch_column(cl_, stream_), "column (init)");
+}
+
+void GpuSolver::build_graph() {
+  // Launch attributes are set on first use outside capture.
+  check(launch_leader(ll_, stream_), "leader");
+  check(launch_column(cl_, stream_), "column");
+  graph_iters_ = 64;
+  cudaGraph_t g = nullptr;
+  check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  for (long long i = 0; i < graph_iters_; ++i) {
+    launch_leader(ll_, stream_);
+    launch_column(cl_, stream_);
+  }
+  check(cudaStreamEndCapture(stream_, &g), "end capture");
+  check(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
+  cudaGraphDestroy(g);
+}
+
+void GpuSolver::run_iterations(long long n) {
+  if (n <= 0) return;
+  if (!graph_) {
+    build_graph();
+    --n;  // build_graph ran one iteration
+  }
+  while (n >= graph_iters_) {
+    check(cudaGraphLaunch(graph_, stream_), "graph launch");
+    n -= graph_iters_;
+  }
+  for (; n > 0; --n) {
+    check(launch_leader(ll_, stream_), "leader");
+    check(launch_column(cl_, stream_), "column");
+  }
+}
+
+void GpuSolver::run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms) {
+  *leader_ms = *column_ms = *total_ms = 0.0;
+  if (n <= 0) return;
+  std::vector<cudaEvent_t> ev(static_cast<size_t>(2 * n + 1));
+  for (auto& e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
+  try {
+    check(cudaEventRecord(ev[0], stream_), "cudaEventRecord");
+    for (long long i = 0; i < n; ++i) {
+      check(launch_leader(ll_, stream_), "leader");
+      check(cudaEventRecord(ev[2 * i + 1], stream_), "cudaEventRecord");
+      check(launch_column(cl_, stream_), "column");
+      check(cudaEventRecord(ev[2 * i + 2], stream_), "cudaEventRecord");
+    }
+    check(cudaEventSynchronize(ev[2 * n]), "cudaEventSynchronize");
+    for (long long i = 0; i < n; ++i) {
+      float a = 0.f, b = 0.f;
+      check(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]), "cudaEventElapsedTime");
+      check(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]), "cudaEventElapsedTime");
+      *leader_ms += a;
+      *column_ms += b;
+    }
+    float t = 0.f;
+    check(cudaEventElapsedTime(&t, ev[0], ev[2 * n]), "cudaEventElapsedTime");
+    *total_ms = t;
+  } catch (...) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+}
+
+void GpuSolver::read_state() {
+  check(launch_finish(ll_, stream_), "finish");
+  check(cudaMemcpyAsync(&h_state_, d_state_, sizeof(IterState), cudaMemcpyDeviceToHost, stream_), "state read");
+  unsigned err = 0;
+  check(cudaMemcpyAsync(&err, d_err_, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_), "error read");
+  check(cudaStreamSynchronize(stream_), "synchronize");
+  if (err) {
+    if (err & (kErrProbe | kErrOverflow))
+      throw McdError(MCD_ERR_OVERFLOW, "The hash table is full. Please increase max_memory or z_threshold.");
+    if (err & kErrEig) throw McdError(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
+    if (err & kErrCandidates) throw McdError(MCD_ERR_NO_CANDIDATES, "The candidate list is empty.");
+    throw McdError(MCD_ERR_CUDA, "device error word " + std::to_string(err));
+  }
+}
+
+mcd_report GpuSolver::report() {
+  read_state();
+  mcd_report r{};
+  r.iteration = h_state_.iter;
+  const dd xz{dd_to_d(h_state_.xz), 0.0};
+  r.energy = dd_to_d(dd_div(xz, h_state_.xx));
+  r.dx_max = h_state_.dx_max;
+  r.x_size = h_state_.x_size;
+  r.z_size = h_state_.z_size;
+  r.cols_size = h_state_.emitted;
+  r.updates = h_state_.updates;
+  r.scale = dd_to_d(h_state_.scale);
+  r.max_residual = h_state_.eig_residual_max;
+  r.z_threshold = zt_;
+  r.emitted_total = h_state_.emitted_total;
+  r.updates_total = h_state_.updates_total;
+  r.occupied = 0;
+  check(cudaMemcpy(&r.occupied, d_occ_, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "occupancy read");
+  r.last_k = h_state_.k_cur;
+  return r;
+}
+
+void GpuSolver::scalars(dd* xx, dd* scale, dd* xz, long long* iter) {
+  read_state();
+  *xx = h_state_.xx;
+  *scale = h_state_.scale;
+  *xz = h_state_.xz;
+  *iter = h_state_.iter;
+}
+
+int GpuSolver::solve(mcd_report_cb cb, void* user) {
+  const bool v = opt_.verbose;
+  if (v) {
+    std::cout << "CDFCI calculation" << std::endl << "-----------------" << std::endl;
+    std::cout << "Hartree Fock determinant occupied spin-orbitals:" << std::endl;
+    for (int so : det_spin_orbitals(ref_, ham_.norb)) std::cout << so << "  ";
+    std::cout << std::endl;
+    std::cout << "Hartree Fock energy: " << std::fixed << std::setprecision(10) << ref_diag_ << std::endl
+              << std::endl;
+  }
+  while (true) {
+    reset();
+    const auto t0 = std::chrono::steady_clock::now();
+    if (v) {
+      std::cout << std::setw(13) << std::left << "Iteration";
+      std::cout << std::setw(18) << std::right << "Energy";
+      std::cout << std::setw(18) << "|dx|_max";
+      std::cout << std::setw(12) << "|x|_0";
+      std::cout << std::setw(12) << "|z|_0";
+      std::cout << std::setw(10) << "|H[I]|_0";
+      std::cout << std::setw(10) << "upds";
+      std::cout << std::setw(10) << "Time";
+      std::cout << std::setw(10) << "scale";
+      std::cout << std::endl;
+    }
+    unsigned long long last_z = 0;
+    bool restart = false;
+    double energy = 0.0;
+    const long long chunks = opt_.num_iterations / opt_.report_interval;
+    for (long long c = 0; c < chunks; ++c) {
+      run_iterations(opt_.report_interval);
+      mcd_report r = report();
+      r.time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      energy = r.energy;
+      if (v) {
+        std::cout << std::setw(13) << std::left << (c + 1) * opt_.report_interval;
+        std::cout << std::setw(18) << std::right << std::fixed << std::setprecision(10) << r.energy;
+        std::cout << std::setw(18) << std::scientific << std::setprecision(4) << r.dx_max;
+        std::cout << std::setw(12) << r.x_size;
+        std::cout << std::setw(12) << r.z_size;
+        std::cout << std::setw(10) << r.cols_size;
+        std::cout << std::setw(10) << r.updates;
+        std::cout << std::setw(10) << std::fixed << std::setprecision(2) << r.time_s;
+        std::cout << std::setw(10) << std::fixed << std::setprecision(6) << r.scale;
+        std::cout << std::endl;
+        std::printf("[LOG] max residual: %e, subspace problem: %s\n", r.max_residual,
+                    h_state_.last_branch == 2 ? "k x k" : "(k+1) x (k+1)");
+        std::fflush(stdout);
+      }
+      if (cb && cb(&r, user) != 0) {
+        result_energy_ = energy;
+        return MCD_STOPPED;
+      }
+      // z_threshold search (src/solver.h:802-810).
+      if (opt_.z_threshold_search) {
+        int ncand = 0;
+        for (int i = 0; i < h_state_.k_cur; ++i) ncand += h_state_.cand_n[i];
+        const double inc = 1000.0 * static_cast<double>(r.z_size - last_z) / std::max(ncand, 1) /
+                           static_cast<double>(opt_.report_interval);
+        if (inc >= 1.0 && static_cast<double>(r.z_size) > 0.7 * static_cast<double>(max_size_)) {
+          restart = true;
+          break;
+        }
+      }
+      last_z = r.z_size;
+      if (static_cast<double>(r.z_size) > 0.79 * static_cast<double>(max_size_))
+        throw McdError(MCD_ERR_OVERFLOW, "The hash table is full. Please increase max_memory or z_threshold.");
+    }
+    if (restart) {
+      zt_ *= 2.0;
+      if (v)
+        std::cout << "z_threshold_search: z_threshold is too small. Increase z_threhold to " << std::scientific
+                  << std::setprecision(2) << zt_ << " and restart." << std::endl;
+      continue;
+    }
+    result_energy_ = energy;
+    return MCD_OK;
+  }
+}
+
+std::vector<std::pair<Det, double>> GpuSolver::column(Det d) {
+  const int cap = entries_;
+  uint64_t* da = device_alloc<uint64_t>(cap, "debug");
+  uint64_t* db = device_alloc<uint64_t>(cap, "debug");
+  double* dv = device_alloc<double>(cap, "debug");
+  int* dn = device_alloc<int>(1, "debug");
+  std::vector<std::pair<Det, double>> out;
+  try {
+    check(debug_column(hd_, d, diagonal_element(ham_, d), da, db, dv, cap, dn, stream_), "debug column");
+    int n = 0;
+    check(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy");
+    check(cudaStreamSynchronize(stream_), "sync");
+    n = std::min(n, cap);
+    std::vector<uint64_t> ha(n), hb(n);
+    std::vector<double> hv(n);
+    if (n) {
+      check(cudaMemcpy(ha.data(), da, n * 8, cudaMemcpyDeviceToHost), "copy");
+      check(cudaMemcpy(hb.data(), db, n * 8, cudaMemcpyDeviceToHost), "copy");
+      check(cudaMemcpy(hv.data(), dv, n * 8, cudaMemcpyDeviceToHost), "copy");
+    }
+    for (int i = 0; i < n; ++i) out.push_back({Det{ha[i], hb[i]}, hv[i]});
+  } catch (...) {
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dv);
+    cudaFree(dn);
+    throw;
+  }
+  cudaFree(da);
+  cudaFree(db);
+  cudaFree(dv);
+  cudaFree(dn);
+  return out;
+}
+
+std::vector<double> GpuSolver::hsub(const std::vector<Det>& dets) {
+  const int k = static_cast<int>(dets.size());
+  Det* dd_ = device_alloc<Det>(std::max(k, 1), "debug");
+  double* dh = device_alloc<double>(std::max(k * k, 1), "debug");
+  std::vector<double> out(static_cast<size_t>(k) * k);
+  check(cudaMemcpyAsync(dd_, dets.data(), k * sizeof(Det), cudaMemcpyHostToDevice, stream_), "copy");
+  check(debug_hsub(hd_, dd_, k, dh, stream_), "debug hsub");
+  check(cudaMemcpyAsync(out.data(), dh, out.size() * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "sync");
+  cudaFree(dd_);
+  cudaFree(dh);
+  return out;
+}
+
+void GpuSolver::table_sums(dd* xx, dd* xz, unsigned long long* occupied) {
+  read_state();
+  const int nb = 148 * 4;
+  dd* dp = device_alloc<dd>(2 * nb, "debug");
+  unsigned long long* dc = device_alloc<unsigned long long>(1, "debug");
+  std::vector<dd> hp(2 * nb);
+  unsigned long long c = 0;
+  check(cudaMemsetAsync(dc, 0, 8, stream_), "memset");
+  check(launch_table_sums(d_slots_, capacity_, dp, dc, nb, stream_), "table sums");
+  check(cudaMemcpyAsync(hp.data(), dp, hp.size() * sizeof(dd), cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaMemcpyAsync(&c, dc, 8, cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "sync");
+  cudaFree(dp);
+  cudaFree(dc);
+  dd a{0, 0}, b{0, 0};
+  for (int i = 0; i < nb; ++i) {
+    a = dd_add(a, hp[2 * i]);
+    b = dd_add(b, hp[2 * i + 1]);
+  }
+  *xx = a;
+  *xz = b;
+  *occupied = c;
+}
+
+std::vector<std::pair<Det, double>> GpuSolver::picked() {
+  read_state();
+  std::vector<std::pair<Det, double>> out;
+  for (int i = 0; i < h_state_.k_cur; ++i) out.push_back({h_state_.det[i], h_state_.dx[i]});
+  return out;
+}
+
+}  // namespace mcd

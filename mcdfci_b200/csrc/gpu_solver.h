@@ -1,0 +1,118 @@
+// GPU solver: owns the device tables, the hash wavefunction and the iteration
+// state, and runs the reference's solve loop (CDFCI<N>::solve,
+// src/solver.h:672-893) as launches on one CUDA stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mcdfci.h"
+#include "fcidump.h"
+#include "hamiltonian.h"
+#include "kernels.h"
+
+namespace mcd {
+
+struct SolverOptions {
+  long long num_iterations = 10;
+  long long report_interval = 1;
+  int k = 1;
+  int m = 100;
+  double z_threshold = 0.0;
+  bool z_threshold_search = false;
+  double max_memory = 0.0;
+  double threshold = 1e-13;
+  std::vector<int> ref_det_occ;
+  int coordinate_pick = MCD_PICK_GCD_GRAD;
+  int coordinate_update = MCD_UPDATE_EIG;
+  int cluster = 0;
+  bool verbose = false;
+  cudaStream_t stream = nullptr;
+  int device = -1;
+};
+
+// Status with a message; thrown inside the library, turned into a return code
+// at the C ABI.
+struct McdError : std::runtime_error {
+  int code;
+  McdError(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
+};
+
+class GpuSolver {
+ public:
+  GpuSolver(const Fcidump& fci, const SolverOptions& opt);
+  ~GpuSolver();
+  GpuSolver(const GpuSolver&) = delete;
+  GpuSolver& operator=(const GpuSolver&) = delete;
+
+  // Full solve with reports and z_threshold_search restarts.
+  int solve(mcd_report_cb cb, void* user);
+  // Initial state with the current z_threshold.
+  void reset();
+  // Enqueue n iterations (asynchronous).
+  void run_iterations(long long n);
+  // Run n iterations with direct launches and a CUDA event between every
+  // two kernels on the solver's stream; waits, and returns the summed
+  // leader-kernel and column-kernel device times and the total (ms).
+  void run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms);
+  // Apply the pending end-of-iteration step, wait, and read the state.
+  mcd_report report();
+
+  double result_energy() const { return result_energy_; }
+  cudaStream_t stream() const { return stream_; }
+  void scalars(dd* xx, dd* scale, dd* xz, long long* iter);
+
+  // Parity / debug.
+  std::vector<std::pair<Det, double>> column(Det d);
+  std::vector<double> hsub(const std::vector<Det>& dets);
+  void table_sums(dd* xx, dd* xz, unsigned long long* occupied);
+  std::vector<std::pair<Det, double>> picked();
+
+  const HamHost& ham() const { return ham_; }
+  Det reference_det() const { return ref_; }
+  long long table_capacity() const { return static_cast<long long>(capacity_); }
+  unsigned long long max_wavefunction_size() const { return max_size_; }
+  int cluster() const { return cluster_; }
+  int entries_per_column() const { return entries_; }
+
+ private:
+  void check(cudaError_t e, const char* what);
+  void release();
+  void read_state();
+  void raise_device_error();
+  void build_graph();
+
+  SolverOptions opt_;
+  HamHost ham_;
+  Det ref_{0, 0};
+  double ref_diag_ = 0.0;
+  int na_ = 0, nb_ = 0, entries_ = 0, cluster_ = 1, n_words_ = 1;
+  size_t capacity_ = 0;             // hash slots (power of two)
+  unsigned long long max_size_ = 0; // reference max_wavefunction_size
+  double zt_ = 0.0;
+  double result_energy_ = 0.0;
+
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  int device_ = 0;
+  void* d_tables_ = nullptr;
+  Slot* d_slots_ = nullptr;
+  IterState* d_state_ = nullptr;
+  double* d_cand_score_ = nullptr;
+  long long* d_cand_slot_ = nullptr;
+  double* d_hsub_ = nullptr;
+  unsigned* d_err_ = nullptr;
+  unsigned long long* d_occ_ = nullptr;
+  HamDev hd_{};
+  TableDev td_{};
+  ColumnLaunch cl_{};
+  LeaderLaunch ll_{};
+  IterState h_state_{};
+
+  cudaGraphExec_t graph_ = nullptr;
+  long long graph_iters_ = 0;
+};
+
+}  // namespace mcd

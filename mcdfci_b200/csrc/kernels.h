@@ -1,0 +1,117 @@
+// Host-visible interface of the sm_100a kernels.
+//
+// One mCDFCI iteration (CDFCI<N>::solve inner loop, src/solver.h:701-759) is
+// two launches on the solver's stream:
+//
+//   leader_kernel   (1 CTA)  finishes the previous iteration's z-update
+//                            (reinsert the exact z of the picked determinants,
+//                            accumulate xz), refetches the candidates, picks the
+//                            next k coordinates, builds H_sub, solves the
+//                            (k+1)x(k+1) eigenproblem and applies x += dx;
+//   column_kernel   (k clusters of C CTAs) generates the k Hamiltonian columns
+//                            and applies z += H_col * dx to the hash table,
+//                            keeping each column's top-m candidates.
+//
+// All scalar solver state lives in IterState in device memory, so iterations
+// run back-to-back without host round trips and can be captured in a graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mcd_types.h"
+
+namespace mcd {
+
+struct IterState {
+  // Solver scalars, carried in double-double (the reference uses __float128).
+  dd xx;       // |x|^2 of the stored (scaled) vector
+  dd scale;    // true coefficients = scale * x
+  dd xz;       // x^T z = x^T H x
+  dd xss;      // xx * scale^2, used for gradients |x*xss + z|
+  double zt;   // z_threshold
+  int n_words; // interleaved words per determinant in the reference layout (tie-break order)
+  int k_req;   // num_of_coordinate
+  int m;       // estimate
+  int pad0;
+  long long iter;  // completed iterations (0 after initialisation)
+
+  // Current iteration (written by the leader, read by the column kernel).
+  int k_cur;
+  int pad1;
+  Det det[kMaxK];
+  long long slot[kMaxK];
+  double dx[kMaxK];
+  double hdiag[kMaxK];
+
+  // Column kernel outputs for the current iteration.
+  double newz[kMaxK];  // exact (H x)_c recomputed over the column
+  double dot[kMaxK];   // sum over the column of dz * x
+  int cand_n[kMaxK];
+
+  // Counters.
+  unsigned long long x_size;        // reference x_size (src/wavefunction.h:425-451)
+  unsigned long long z_size;        // reference z_size: dets inserted by the z-update
+  unsigned long long emitted;       // column entries of the last iteration (|H[I]|_0)
+  unsigned long long updates;       // z updates of the last iteration (upds)
+  unsigned long long occupancy_limit;  // 0.79 * max_wavefunction_size
+  double dx_max;                    // max |dx| of the last iteration
+  double eig_residual_max;          // max ||B v - lambda v|| seen so far
+  int last_branch;                  // 1: (k+1)x(k+1) problem, 2: k x k (first iteration)
+  int pending;                      // 1: the column kernel ran and its z reinsert / xz update is not applied yet
+  unsigned long long emitted_total; // column entries over all iterations
+  unsigned long long updates_total; // z updates over all iterations
+};
+
+struct ColumnLaunch {
+  HamDev ham;
+  TableDev tab;
+  IterState* st;
+  double* cand_score;     // [kMaxK][m]
+  long long* cand_slot;   // [kMaxK][m]
+  int m;
+  int cap_w;              // per-warp candidate buffer capacity (round_up(m,32)+32)
+  int cluster;            // CTAs per column
+  int k_grid;             // columns launched (>= k_cur)
+  int na, nb;             // electrons per spin (fixed by the starting determinant)
+};
+
+struct LeaderLaunch {
+  HamDev ham;
+  TableDev tab;
+  IterState* st;
+  const double* cand_score;
+  const long long* cand_slot;
+  double* hsub_out;       // [kMaxK*kMaxK] last H_sub (row-major, k_cur x k_cur)
+  int m;
+  int k_req;
+};
+
+// Launchers (column_kernel.cu / leader_kernel.cu).
+size_t column_smem_bytes(int m, int nthreads);
+int column_entries(int norb, int na, int nb);
+cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
+cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
+cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStream_t s);
+// Applies the pending end of the last iteration (z reinsert of the picked
+// determinants, xz += dot), so that reported energies and table contents are
+// those after a complete iteration.  Idempotent.
+cudaError_t launch_finish(const LeaderLaunch& a, cudaStream_t s);
+// Table initialisation (all slots empty) and whole-table sums.
+cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s);
+cudaError_t launch_table_sums(const Slot* slots, size_t n, dd* partial, unsigned long long* count, int nblocks,
+                              cudaStream_t s);
+
+// Debug / parity entry points (synchronous).
+// Column of one determinant: writes up to `cap` (a, b, value) entries.
+cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,
+                         double* v_out, int cap, int* n_out, cudaStream_t s);
+cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cudaStream_t s);
+// One eig update on given inputs (device pointers); writes dx[k], xx_scale[0] =
+// new xx, xx_scale[1] = new scale, the branch taken and an error word.
+cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
+                      double* dx, dd* xx_scale, int* branch, unsigned* err, cudaStream_t s);
+size_t leader_smem_bytes(int k, int m);
+
+}  // namespace mcd

@@ -1,0 +1,701 @@
+// Leader kernel: the serial part of one mCDFCI iteration, run by one CTA of
+// 1024 threads between two column-kernel launches.
+//
+//   finish iteration t-1   z[D_c] = new_z_c for the picked D_c (the exact
+//                          recompute that overwrites the accumulated z,
+//                          src/wavefunction.h:557-565); xz += sum_c dot_c
+//                          (src/wavefunction.h:583); occupancy check
+//                          (src/wavefunction.h:594-599)
+//   refetch                (x, z) of every column's candidates from the table
+//                          (src/wavefunction.h:567-575)
+//   pick                   the k distinct determinants with the largest
+//                          |x*xx*scale^2 + z|, ties to the larger determinant
+//                          in the reference order (CoordinatePickGcdGrad,
+//                          src/solver.h:118-143,196-224)
+//   H_sub                  k x k sub-matrix (CDFCI::get_hamiltonian_submatrix,
+//                          src/solver.h:637-670): upper triangle from
+//                          get_off_diagonal(det_i, det_j) for i < j, diagonal
+//                          from get_diagonal (src/hamiltonian.h:252-328)
+//   eig update             dx, scale and xx (CoordinateUpdateEig,
+//                          src/solver.h:333-609)
+//   update_x               x[D_c] += dx_c, xz += z[D_c] * dx_c
+//                          (WaveFunctionCuckoo::update_x, src/wavefunction.h:425-451)
+//   publish                the k picked determinants, dx, H_cc, xx*scale^2
+//                          and scale for the column kernel.
+#include "eig.cuh"
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace mcd {
+namespace {
+
+constexpr int kLT = kEigThreads;  // 1024
+
+// ---------------------------------------------------------------------------
+// Matrix elements between two determinants.
+
+// Single p->r of spin s summed over the occupied spin-orbitals of (a, b) in
+// interleaved order.
+__device__ double single_value_det(const HamDev& h, int s, int p, int r, uint64_t a, uint64_t b) {
+  const int n = h.norb;
+  const size_t base = (static_cast<size_t>(s) * n + p) * n + r;
+  const double* st = h.st + base * h.nso;
+  double v = h.sh[base];
+  uint64_t u = a | b;
+  while (u) {
+    const int q = __ffsll(static_cast<long long>(u)) - 1;
+    u &= u - 1;
+    if ((a >> q) & 1ull) v += st[2 * q];
+    if ((b >> q) & 1ull) v += st[2 * q + 1];
+  }
+  return v;
+}
+
+__device__ __forceinline__ int lowest_bit(uint64_t x) { return __ffsll(static_cast<long long>(x)) - 1; }
+
+// <d2|H|d1> computed from d1's side, as HamiltonianMolecule::get_off_diagonal(d1, d2).
+__device__ double off_diagonal(const HamDev& h, Det d1, Det d2) {
+  const uint64_t da = d1.a ^ d2.a, db = d1.b ^ d2.b;
+  const int na = __popcll(da), nb = __popcll(db);
+  const int n = h.norb;
+  if (na + nb == 2) {
+    if (na == 2) {
+      const int p = lowest_bit(da & d1.a), r = lowest_bit(da & d2.a);
+      if (!((h.spres[p] >> r) & 1ull)) return 0.0;
+      double v = single_value_det(h, 0, p, r, d1.a, d1.b);
+      return sign_alpha(d1.a, d1.b, p, r) ? -v : v;
+    }
+    if (nb == 2) {
+      const int p = lowest_bit(db & d1.b), r = lowest_bit(db & d2.b);
+      if (!((h.spres[n + p] >> r) & 1ull)) return 0.0;
+      double v = single_value_det(h, 1, p, r, d1.a, d1.b);
+      return sign_beta(d1.a, d1.b, p, r) ? -v : v;
+    }
+    return 0.0;
+  }
+  if (na + nb == 4) {
+    const size_t np = static_cast<size_t>(h.npair);
+    if (na == 4) {
+      uint64_t o = da & d1.a, v = da & d2.a;
+      const int p = lowest_bit(o);
+      o &= o - 1;
+      const int q = lowest_bit(o);
+      const int r = lowest_bit(v);
+      v &= v - 1;
+      const int s = lowest_bit(v);
+      const double val = h.vss[static_cast<size_t>(pair_index(p, q)) * np + pair_index(r, s)];
+      return sign_aa(d1.a, d1.b, p, q, r, s) ? -val : val;
+    }
+    if (nb == 4) {
+      uint64_t o = db & d1.b, v = db & d2.b;
+      const int p = lowest_bit(o);
+      o &= o - 1;
+      const int q = lowest_bit(o);
+      const int r = lowest_bit(v);
+      v &= v - 1;
+      const int s = lowest_bit(v);
+      const double val = h.vss[(np + pair_index(p, q)) * np + pair_index(r, s)];
+      return sign_bb(d1.a, d1.b, p, q, r, s) ? -val : val;
+    }
+    if (na == 2 && nb == 2) {
+      const int pa = lowest_bit(da & d1.a), ra = lowest_bit(da & d2.a);
+      const int pb = lowest_bit(db & d1.b), sb = lowest_bit(db & d2.b);
+      const double val = h.wab[((static_cast<size_t>(pa) * n + pb) * n + ra) * n + sb];
+      return sign_ab(d1.a, d1.b, pa, ra, pb, sb) ? -val : val;
+    }
+  }
+  return 0.0;
+}
+
+// Diagonal element by one warp (lane-partial sums, fixed reduction order).
+// occ: 128-byte per-warp scratch.
+__device__ double diagonal_warp(const HamDev& h, Det d, unsigned char* occ) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  int nocc = 0;
+  for (int j = 0; j < 4; ++j) {
+    const int s = lane + 32 * j;
+    const int p = s >> 1;
+    const bool o = p < h.norb && ((((s & 1) ? d.b : d.a) >> p) & 1ull);
+    const unsigned m = __ballot_sync(~0u, o);
+    if (o) occ[nocc + __popc(m & lt)] = static_cast<unsigned char>(s);
+    nocc += __popc(m);
+  }
+  __syncwarp();
+  double v = 0.0;
+  for (int x = lane; x < nocc; x += 32) {
+    const int i = occ[x];
+    double t = h.hdiag[i];
+    const double* row = h.d2 + static_cast<size_t>(i) * h.nso;
+    for (int y = x + 1; y < nocc; ++y) t += row[occ[y]];
+    v += t;
+  }
+  v = warp_sum(v);
+  __syncwarp();
+  return __shfl_sync(~0u, v, 0) + h.ecore;
+}
+
+__device__ __forceinline__ double score_of(double x, double z, dd xss) {
+  if (x == 0.0) return fabs(z);
+  const dd t = dd_add_d(dd_mul_d(xss, x), z);
+  return fabs(t.hi + t.lo);
+}
+
+// ---------------------------------------------------------------------------
+// Eig update.  Inputs in shared memory: x[k], z[k]; H in global memory
+// (row-major k x k, symmetric).  Outputs dx[k] (shared), new xx / scale.
+
+struct EigResult {
+  dd xx, scale;
+  int branch;
+  bool ok;
+  double resid;
+};
+
+__device__ EigResult eig_update(const double* Hg, int k, const double* x, const double* z, dd xx, dd xz,
+                                double* dx, double* smem_d) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ double s_b00, s_y1;
+  __shared__ dd s_red[32];
+  __shared__ double s_redd[32];
+  __shared__ int s_branch;
+  __shared__ int s_ibest;
+  EigResult res;
+
+  // x'x, x'z, Hx, x'Hx in double-double, rounded where the reference works in double.
+  double* Hx = smem_d;  // [k]
+  for (int r = warp; r < k; r += 32) {
+    dd s{0.0, 0.0};
+    for (int c = lane; c < k; c += 32) s = dd_add(s, dd_two_prod(Hg[r * k + c], x[c]));
+    s = warp_sum_dd(s);
+    if (lane == 0) Hx[r] = dd_to_d(s);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    dd sxx{0, 0}, sxz{0, 0}, sxhx{0, 0};
+    for (int i = lane; i < k; i += 32) {
+      sxx = dd_add(sxx, dd_two_prod(x[i], x[i]));
+      sxz = dd_add(sxz, dd_two_prod(x[i], z[i]));
+      sxhx = dd_add(sxhx, dd_two_prod(x[i], Hx[i]));
+    }
+    sxx = warp_sum_dd(sxx);
+    sxz = warp_sum_dd(sxz);
+    sxhx = warp_sum_dd(sxhx);
+    if (lane == 0) {
+      const double xTx = dd_to_d(sxx), xTz = dd_to_d(sxz), xTHx = dd_to_d(sxhx);
+      const double yy = dd_to_d(dd_add_d(xx, -xTx));
+      s_branch = fabs(yy) > 1e-14 ? 1 : 2;
+      if (s_branch == 1) {
+        const double y1 = sqrt(yy);
+        dd num = dd_add_d(dd_add_d(xz, -2.0 * xTz), xTHx);
+        s_b00 = dd_to_d(dd_div_d(num, yy));
+        s_y1 = y1;
+      }
+    }
+  }
+  __syncthreads();
+  const int branch = s_branch;
+  const int n = branch == 1 ? k + 1 : k;
+  const int off = branch == 1 ? 1 : 0;
+  const double y1 = s_y1;
+
+  // Scratch layout after Hx (k doubles).
+  double* base = smem_d + ((k + 1) & ~1) + 2;
+  EigScratch ws;
+  ws.lda = n;
+  ws.A = base;
+  ws.d = ws.A + static_cast<size_t>(n) * n;
+  ws.e = ws.d + n;
+  ws.e2 = ws.e + n;
+  ws.beta = ws.e2 + n;
+  ws.hv = ws.beta + n;
+  ws.p = ws.hv + n;
+  ws.y = ws.p + n;
+  double* bvec = ws.y + n;   // [n] first row of B (branch 1)
+  double* vhi = bvec + n;    // [n] normalised eigenvector, hi part
+  double* vlo = vhi + n;     // [n] lo part
+  ws.part = vlo + n;         // [32]
+  ws.scal = ws.part + 32;    // [8]
+  ws.ibest = &s_ibest;
+
+  // Build B.
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - r * n;
+    double v;
+    if (r >= off && c >= off) {
+      const int i = r - off, j = c - off;
+      v = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];  // upper triangle, as dsyevr UPLO='L' column-major
+    } else if (r == 0 && c == 0) {
+      v = s_b00;
+    } else {
+      const int i = (r == 0 ? c : r) - 1;
+      v = (z[i] - Hx[i]) / y1;
+    }
+    ws.A[idx] = v;
+    if (r == 0) bvec[c] = v;
+  }
+  __syncthreads();
+
+  smallest_eigvec(ws, n);
+
+  // Normalise in double-double; fix the sign.
+  if (warp == 0) {
+    dd nrm{0, 0};
+    double sgn = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      nrm = dd_add(nrm, dd_two_prod(ws.y[i], ws.y[i]));
+      if (branch == 2) sgn += ws.y[i] * x[i];
+    }
+    nrm = warp_sum_dd(nrm);
+    sgn = warp_sum(sgn);
+    nrm = dd{__shfl_sync(~0u, nrm.hi, 0), __shfl_sync(~0u, nrm.lo, 0)};
+    sgn = __shfl_sync(~0u, sgn, 0);
+    const double flip = (branch == 1) ? (ws.y[0] < 0.0 ? -1.0 : 1.0) : (sgn < 0.0 ? -1.0 : 1.0);
+    const dd inv = dd_div(dd{flip, 0.0}, dd_sqrt(nrm));
+    for (int i = lane; i < n; i += 32) {
+      const dd vi = dd_mul_d(inv, ws.y[i]);
+      vhi[i] = vi.hi;
+      vlo[i] = vi.lo;
+    }
+  }
+  __syncthreads();
+
+  // Rayleigh quotient v'Bv in double-double.
+  {
+    dd acc{0, 0};
+    for (int r = warp; r < n; r += 32) {
+      dd s{0, 0};
+      for (int c = lane; c < n; c += 32) {
+        double brc;
+        if (r >= off && c >= off) {
+          const int i = r - off, j = c - off;
+          brc = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];
+        } else {
+          brc = bvec[r == 0 ? c : r];
+        }
+        s = dd_add(s, dd_mul_d(dd{vhi[c], vlo[c]}, brc));
+      }
+      s = warp_sum_dd(s);
+      s = dd{__shfl_sync(~0u, s.hi, 0), __shfl_sync(~0u, s.lo, 0)};
+      acc = dd_add(acc, dd_mul(s, dd{vhi[r], vlo[r]}));
+    }
+    if (lane == 0) s_red[warp] = acc;
+  }
+  __syncthreads();
+  __shared__ dd s_rq;
+  if (tid == 0) {
+    dd t{0, 0};
+    for (int w = 0; w < 32; ++w) t = dd_add(t, s_red[w]);
+    s_rq = t;
+  }
+  __syncthreads();
+  const dd rq = s_rq;
+  const double lam = dd_to_d(rq);
+  // Residual ||B v - lambda v|| (diagnostic, reported like the reference's max residual).
+  {
+    double acc = 0.0;
+    for (int r = warp; r < n; r += 32) {
+      double s = 0.0;
+      for (int c = lane; c < n; c += 32) {
+        double brc;
+        if (r >= off && c >= off) {
+          const int i = r - off, j = c - off;
+          brc = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];
+        } else {
+          brc = bvec[r == 0 ? c : r];
+        }
+        s += brc * vhi[c];
+      }
+      s = warp_sum(s);
+      const double t = s - lam * vhi[r];
+      acc += t * t;
+    }
+    if (lane == 0) s_redd[warp] = acc;
+  }
+  __syncthreads();
+  double rr = 0.0;
+  for (int w = 0; w < 32; ++w) rr += s_redd[w];
+  res.resid = sqrt(rr);
+  res.branch = branch;
+  res.ok = true;
+
+  if (branch == 1) {
+    const dd lq = dd_neg(rq);
+    const dd v0{vhi[0], vlo[0]};
+    const dd gamma = dd_div_d(v0, y1);
+    res.ok = lq.hi > 0.0 && gamma.hi != 0.0 && isfinite(lq.hi) && isfinite(gamma.hi);
+    const dd sc = dd_mul(gamma, dd_sqrt(lq));
+    res.scale = sc;
+    res.xx = dd_div(lq, dd_mul(sc, sc));
+    for (int i = tid; i < k; i += blockDim.x) {
+      const dd q = dd_div(dd{vhi[i + 1], vlo[i + 1]}, gamma);
+      dx[i] = dd_to_d(dd_add_d(q, -x[i]));
+    }
+  } else {
+    res.ok = lam < 0.0 && isfinite(lam);
+    const double sq = sqrt(-lam);
+    res.xx = dd{-lam, 0.0};
+    res.scale = dd{1.0, 0.0};
+    for (int i = tid; i < k; i += blockDim.x) dx[i] = (vhi[i] + vlo[i]) * sq - x[i];
+  }
+  __syncthreads();
+  for (int i = tid; i < k; i += blockDim.x)
+    if (!isfinite(dx[i])) res.ok = false;
+  res.ok = __syncthreads_and(res.ok ? 1 : 0) != 0;
+  return res;
+}
+
+// ---------------------------------------------------------------------------
+
+// End of iteration t (src/wavefunction.h:557-565,583): z[D_c] = new_z_c for
+// the picked determinants, then xz += sum_c dot_c.  Block-wide.
+__device__ void finish_iteration(IterState* S, const TableDev& T, bool pending) {
+  if (!pending) return;
+  const int k = S->k_cur;
+  if (static_cast<int>(threadIdx.x) < k) {
+    Slot* sp = T.slots + S->slot[threadIdx.x];
+    sp->z = S->newz[threadIdx.x];
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dd xz = S->xz;
+    for (int c = 0; c < k; ++c) xz = dd_add_d(xz, S->dot[c]);
+    S->xz = xz;
+    S->pending = 0;
+  }
+}
+
+__global__ void finish_kernel(LeaderLaunch L) {
+  finish_iteration(L.st, L.tab, L.st->pending != 0);
+}
+
+__global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_off[kMaxK + 1];
+  __shared__ int s_k, s_R;
+  __shared__ unsigned s_err;
+  __shared__ long long s_slot[kMaxK];
+  __shared__ Det s_det[kMaxK];
+  __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
+  __shared__ unsigned char s_occ[32][128];
+  __shared__ unsigned long long s_newx;
+
+  IterState* S = L.st;
+  const TableDev& T = L.tab;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m = L.m;
+
+  // 1. Finish the previous iteration (unless finish_kernel already did).
+  const int kprev = S->k_cur;
+  const bool pending = S->pending != 0;
+  finish_iteration(S, T, pending);
+  if (tid == 0) {
+    if (*T.n_occupied > S->occupancy_limit) atomicOr(T.err, kErrOverflow);
+    s_err = *reinterpret_cast<volatile unsigned*>(T.err);
+    s_newx = 0;
+  }
+  if (warp == 0) {
+    // Exclusive prefix of the candidate counts over the columns.
+    int run = 0;
+    for (int base = 0; base < kMaxK; base += 32) {
+      const int cc = (base + lane < kprev) ? S->cand_n[base + lane] : 0;
+      int incl = cc;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(~0u, incl, o);
+        if (lane >= o) incl += t;
+      }
+      s_off[base + lane] = run + incl - cc;
+      run += __shfl_sync(~0u, incl, 31);
+    }
+    if (lane == 0) {
+      s_off[kMaxK] = run;
+      s_R = run;
+    }
+  }
+  __syncthreads();
+  if (s_err != 0u || s_R == 0) {
+    if (tid == 0) {
+      if (s_R == 0 && s_err == 0u) atomicOr(T.err, kErrCandidates);
+      S->k_cur = 0;
+    }
+    return;
+  }
+
+  // 2. Refetch the candidates and score them.
+  const int R = s_R;
+  int P = 1;
+  while (P < R) P <<= 1;
+  double* sc = reinterpret_cast<double*>(smem);
+  int* ix = reinterpret_cast<int*>(sc + P);
+  const dd xss = S->xss;
+  for (int r = tid; r < P; r += kLT) {
+    if (r < R) {
+      int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_off[mid] <= r) lo = mid; else hi = mid;
+      }
+      const int j = r - s_off[lo];
+      const int flat = lo * m + j;
+      const long long slot = L.cand_slot[flat];
+      const Slot* sp = T.slots + slot;
+      const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
+      sc[r] = score_of(x, z, xss);
+      ix[r] = flat;
+    } else {
+      sc[r] = -1.0;
+      ix[r] = -1;
+    }
+  }
+  __syncthreads();
+
+  // 3. Bitonic sort, highest priority first: larger score, then the larger
+  //    determinant in the reference order.
+  const int nwords = S->n_words;
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = tid; t < (P >> 1); t += kLT) {
+        const int i = 2 * stride * (t / stride) + (t % stride);
+        const int j = i + stride;
+        const double si = sc[i], sj = sc[j];
+        bool jfirst;  // j has higher priority than i
+        if (si != sj) {
+          jfirst = sj > si;
+        } else if (ix[i] < 0 || ix[j] < 0) {
+          jfirst = false;
+        } else {
+          const long long a = L.cand_slot[ix[i]], b = L.cand_slot[ix[j]];
+          if (a == b) {
+            jfirst = false;
+          } else {
+            uint64_t ia, ib, ja, jb;
+            load_key(T.slots + a, ia, ib);
+            load_key(T.slots + b, ja, jb);
+            jfirst = det_ref_compare(ja, jb, ia, ib, nwords) > 0;
+          }
+        }
+        const bool up = (i & size) == 0;
+        if (jfirst == up) {
+          sc[i] = sj;
+          sc[j] = si;
+          const int tmp = ix[i];
+          ix[i] = ix[j];
+          ix[j] = tmp;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  // 4. First k distinct determinants (duplicates are adjacent).
+  if (warp == 0) {
+    int got = 0;
+    long long prev = -1;
+    for (int base = 0; base < R && got < L.k_req; base += 32) {
+      const int r = base + lane;
+      const long long slot = r < R ? L.cand_slot[ix[r]] : -1;
+      const long long left = __shfl_up_sync(~0u, slot, 1);
+      const long long before = lane == 0 ? prev : left;
+      const bool fresh = r < R && slot != before;
+      const unsigned fm = __ballot_sync(~0u, fresh);
+      const int pos = got + __popc(fm & lanemask_lt());
+      if (fresh && pos < L.k_req) s_slot[pos] = slot;
+      got += __popc(fm);
+      prev = __shfl_sync(~0u, slot, 31);
+    }
+    if (lane == 0) s_k = got < L.k_req ? got : L.k_req;
+  }
+  __syncthreads();
+  const int k = s_k;
+  if (tid < k) {
+    const Slot* sp = T.slots + s_slot[tid];
+    uint64_t a, b;
+    load_key(sp, a, b);
+    s_det[tid] = Det{a, b};
+    s_x[tid] = load_relaxed(&sp->x);
+    s_z[tid] = load_relaxed(&sp->z);
+  }
+  __syncthreads();
+
+  // 5. H_sub.
+  double* Hg = L.hsub_out;
+  for (int t = tid; t < k * k; t += kLT) {
+    const int i = t / k, j = t - i * k;
+    if (i < j) {
+      const double v = off_diagonal(L.ham, s_det[i], s_det[j]);
+      Hg[i * k + j] = v;
+      Hg[j * k + i] = v;
+    }
+  }
+  for (int i = warp; i < k; i += 32) {
+    const double v = diagonal_warp(L.ham, s_det[i], s_occ[warp]);
+    if (lane == 0) Hg[i * k + i] = v;
+  }
+  __threadfence_block();
+  __syncthreads();
+
+  // 6. Eig update.
+  const EigResult er = eig_update(Hg, k, s_x, s_z, S->xx, S->xz, s_dx, reinterpret_cast<double*>(smem));
+  if (!er.ok) {
+    if (tid == 0) {
+      atomicOr(T.err, kErrEig);
+      S->k_cur = 0;
+    }
+    return;
+  }
+
+  // 7. update_x.
+  if (tid < k) {
+    Slot* sp = T.slots + s_slot[tid];
+    const double x0 = s_x[tid];
+    sp->x = x0 + s_dx[tid];
+    if (x0 == 0.0) atomicAdd(&s_newx, 1ull);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    dd xz = S->xz;
+    double mx = 0.0;
+    for (int i = 0; i < k; ++i) {
+      xz = dd_add_d(xz, s_z[i] * s_dx[i]);
+      mx = fmax(mx, fabs(s_dx[i]));
+    }
+    S->xz = xz;
+    S->xx = er.xx;
+    S->scale = er.scale;
+    S->xss = dd_mul(er.xx, dd_mul(er.scale, er.scale));
+    S->x_size += s_newx;
+    S->dx_max = mx;
+    S->eig_residual_max = fmax(S->eig_residual_max, er.resid);
+    S->last_branch = er.branch;
+    S->emitted = 0;
+    S->updates = 0;
+    S->iter += 1;
+    S->k_cur = k;
+    S->pending = 1;
+  }
+  // 8. Publish.
+  if (tid < k) {
+    S->det[tid] = s_det[tid];
+    S->slot[tid] = s_slot[tid];
+    S->dx[tid] = s_dx[tid];
+    S->hdiag[tid] = Hg[tid * k + tid];
+  }
+}
+
+// Initial state (CDFCI::solve, src/solver.h:862-873): x = e_ref, z = H[:,ref]
+// through one column update with dx = 1, xx = scale = 1, xz = 0.
+__global__ void init_kernel(LeaderLaunch L, Det ref, double ref_diag) {
+  IterState* S = L.st;
+  bool inserted = false;
+  const long long slot = table_upsert(L.tab, ref.a, ref.b, inserted);
+  if (slot < 0) {
+    S->k_cur = 0;
+    return;
+  }
+  Slot* sp = L.tab.slots + slot;
+  const double x0 = sp->x;
+  sp->x = x0 + 1.0;
+  S->x_size = (x0 == 0.0) ? 1 : 0;
+  S->xx = dd{1.0, 0.0};
+  S->scale = dd{1.0, 0.0};
+  S->xz = dd_add_d(dd{0.0, 0.0}, sp->z * 1.0);
+  S->xss = dd{1.0, 0.0};
+  S->k_cur = 1;
+  S->det[0] = ref;
+  S->slot[0] = slot;
+  S->dx[0] = 1.0;
+  S->hdiag[0] = ref_diag;
+  S->emitted = 0;
+  S->updates = 0;
+  S->z_size = 0;
+  S->iter = 0;
+  S->dx_max = 1.0;
+  S->eig_residual_max = 0.0;
+  S->last_branch = 0;
+  S->pending = 1;
+}
+
+__global__ void debug_hsub_kernel(HamDev h, const Det* dets, int k, double* H) {
+  __shared__ unsigned char s_occ[32][128];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int t = tid; t < k * k; t += blockDim.x) {
+    const int i = t / k, j = t - i * k;
+    if (i != j) H[t] = off_diagonal(h, dets[i], dets[j]);
+  }
+  for (int i = warp; i < k; i += blockDim.x / 32) {
+    const double v = diagonal_warp(h, dets[i], s_occ[warp]);
+    if (lane == 0) H[i * k + i] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, const double* H, const double* x,
+                                                           const double* z, dd xx, dd xz, double* dx,
+                                                           dd* out, int* branch, unsigned* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    s_x[i] = x[i];
+    s_z[i] = z[i];
+  }
+  __syncthreads();
+  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem));
+  for (int i = threadIdx.x; i < k; i += blockDim.x) dx[i] = s_dx[i];
+  if (threadIdx.x == 0) {
+    out[0] = er.xx;
+    out[1] = er.scale;
+    *branch = er.branch;
+    *err = er.ok ? 0u : kErrEig;
+  }
+}
+
+}  // namespace
+
+size_t leader_smem_bytes(int k, int m) {
+  size_t P = 1;
+  while (P < static_cast<size_t>(k) * m) P <<= 1;
+  const size_t pick = P * (sizeof(double) + sizeof(int));
+  const size_t n = static_cast<size_t>(k) + 1;
+  const size_t eig = (n * n + 12 * n + 128) * sizeof(double);
+  return pick > eig ? pick : eig;
+}
+
+cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s) {
+  const size_t bytes = leader_smem_bytes(a.k_req, a.m);
+  static size_t configured = 0;
+  if (bytes > configured) {
+    cudaError_t e = cudaFuncSetAttribute(leader_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    configured = bytes;
+  }
+  leader_kernel<<<1, kLT, bytes, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStream_t s) {
+  init_kernel<<<1, 1, 0, s>>>(a, hf, hf_diag);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish(const LeaderLaunch& a, cudaStream_t s) {
+  finish_kernel<<<1, kMaxK, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cudaStream_t s) {
+  debug_hsub_kernel<<<1, 256, 0, s>>>(h, dets, k, hsub);
+  return cudaGetLastError();
+}
+
+cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
+                      double* dx, dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
+  const size_t bytes = leader_smem_bytes(k, 1);
+  cudaError_t e = cudaFuncSetAttribute(debug_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(bytes));
+  if (e != cudaSuccess) return e;
+  debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err);
+  return cudaGetLastError();
+}
+
+}  // namespace mcd

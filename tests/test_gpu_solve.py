@@ -1,0 +1,129 @@
+"""End-to-end GPU solves against the reference's converged energies
+(tests/golden/energies.json, printed by the reference solver built from its
+sources) and against dense FP64 diagonalisation, plus the solver's invariants
+and error paths.  Energies: within 1e-6 Ha of the reference, within 1e-8 Ha
+of the dense eigenvalue."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle.oracle import Oracle
+
+import mcdfci_b200 as m
+
+pytestmark = pytest.mark.gpu
+
+ENERGIES = load_golden("energies.json")
+
+
+def _solve(path, **kw):
+    opts = dict(threshold=0.0, coordinate_update="eig")
+    opts.update(kw)
+    s = m.CDFCI(m.Fcidump(path), **opts)
+    e = s.solve()
+    return s, e
+
+
+def test_h2o_matches_reference(fcidumps):
+    s, e = _solve(fcidumps["h2o_sto3g"], num_iterations=20000, report_interval=1000, max_memory=0.005,
+                  num_of_coordinate=8, estimate=8)
+    assert abs(e - ENERGIES["h2o_sto3g k8 m8 20000it"]) < 1e-6
+    assert len(s.reports) == 20
+    assert [r["iteration"] for r in s.reports] == [1000 * (i + 1) for i in range(20)]
+    xs = [r["x_size"] for r in s.reports]
+    zs = [r["z_size"] for r in s.reports]
+    assert xs == sorted(xs) and zs == sorted(zs)
+    assert s.reports[-1]["z_size"] <= 61440  # FCI space of H2O/STO-3G minus the reference det
+
+
+def test_h2o_k4_m6_matches_reference(fcidumps):
+    _, e = _solve(fcidumps["h2o_sto3g"], num_iterations=40000, report_interval=4000, max_memory=0.005,
+                  num_of_coordinate=4, estimate=6)
+    assert abs(e - ENERGIES["h2o_sto3g k4 m6 40000it"]) < 1e-6
+
+
+def test_h2o_z_threshold_matches_reference(fcidumps):
+    _, e = _solve(fcidumps["h2o_sto3g"], num_iterations=20000, report_interval=2000, max_memory=0.005,
+                  num_of_coordinate=8, estimate=8, z_threshold=1e-5)
+    assert abs(e - ENERGIES["h2o_sto3g k8 m8 20000it z_threshold=1e-5"]) < 1e-6
+
+
+def _dense_n7(path):
+    o = Oracle(path, 0.0)
+    from itertools import combinations
+
+    dets = [(sum(1 << p for p in a), sum(1 << p for p in b)) for a in combinations(range(7), 5)
+            for b in combinations(range(7), 5)]
+    idx = {d: i for i, d in enumerate(dets)}
+    H = np.zeros((len(dets), len(dets)))
+    for d in dets:
+        cd, cv = o.column_ab(*d)
+        for e, v in zip(cd, cv):
+            H[idx[e], idx[d]] = v
+    return np.linalg.eigvalsh(H)[0]
+
+
+def test_n7_matches_dense(fcidumps):
+    e0 = _dense_n7(fcidumps["n7_5a5b"])
+    _, e = _solve(fcidumps["n7_5a5b"], num_iterations=3000, report_interval=1000, max_memory=0.001,
+                  num_of_coordinate=8, estimate=8)
+    assert abs(e - e0) < 1e-8
+    assert abs(e - ENERGIES["n7_5a5b seed0 k8 m8 1000it"]) < 1e-6
+
+
+def test_incremental_scalars_match_table(fcidumps):
+    """xx and xz carried by the iteration equal sum x^2 and sum x*z over the
+    hash table (WaveFunctionCuckoo::debug_calculate_xx_xz, src/wavefunction.h:640-667)."""
+    s = m.CDFCI(m.Fcidump(fcidumps["h2o_sto3g"]), threshold=0.0, max_memory=0.005, num_of_coordinate=8,
+                estimate=8)
+    s.reset()
+    for n in (1, 10, 300):
+        s.run_iterations(n)
+        sc = s.scalars()
+        t = s.table_sums()
+        xx, txx = sum(sc["xx"]), sum(t["xx"])
+        xz, txz = sum(sc["xz"]), sum(t["xz"])
+        assert abs(xx - txx) <= 1e-12 * abs(xx)
+        assert abs(xz - txz) <= 1e-10 * abs(xz)
+
+
+def test_overflow_is_reported_not_hung(synth_fcidumps):
+    s = m.CDFCI(m.Fcidump(synth_fcidumps["n24_6a6b"]), threshold=0.0, max_memory=1e-4, num_of_coordinate=8,
+                estimate=8, num_iterations=50, report_interval=10)
+    with pytest.raises(m.McdError) as e:
+        s.solve()
+    assert e.value.code == m.MCD_ERR_OVERFLOW
+    assert "hash table is full" in e.value.message
+
+
+def test_callback_can_stop(fcidumps):
+    s = m.CDFCI(m.Fcidump(fcidumps["h2o_sto3g"]), threshold=0.0, max_memory=0.005, num_of_coordinate=8,
+                estimate=8, num_iterations=5000, report_interval=100)
+    s.solve(callback=lambda r: r["iteration"] >= 300)
+    assert s.reports[-1]["iteration"] == 300
+
+
+def test_cli_on_input_deck(fcidumps, tmp_path):
+    deck = tmp_path / "input.json"
+    deck.write_text(
+        '{"hamiltonian": {"fcidump_path": "%s", "threshold": 0.0},'
+        ' "solver": {"cdfci": {"num_iterations": 20000, "report_interval": 1000, "z_threshold": 0,'
+        ' "z_threshold_search": false, "max_memory": 0.005, "coordinate_pick": "gcd_grad",'
+        ' "coordinate_update": "eig", "num_of_coordinate": 8, "estimate": 8}}}' % fcidumps["h2o_sto3g"]
+    )
+    res = subprocess.run([m.CLI_PATH, str(deck)], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr
+    rows = [l for l in res.stdout.splitlines() if re.match(r"^\d+\s+-?\d+\.\d+", l)]
+    assert len(rows) == 20
+    assert abs(float(rows[-1].split()[1]) - ENERGIES["h2o_sto3g k8 m8 20000it"]) < 1e-6
+
+
+def test_cli_error_exit(tmp_path):
+    deck = tmp_path / "input.json"
+    deck.write_text('{"hamiltonian": {"fcidump_path": "/nonexistent"}, "solver": {"cdfci": {"max_memory": 1}}}')
+    res = subprocess.run([m.CLI_PATH, str(deck)], capture_output=True, text=True, timeout=60)
+    assert res.returncode == 1 and "ERROR:" in res.stderr

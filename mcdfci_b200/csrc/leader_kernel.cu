@@ -441,7 +441,8 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
       const long long slot = L.cand_slot[flat];
       const Slot* sp = T.slots + slot;
       const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
-      sc[r] = score_of(x, z, xss);
+      const double g = score_of(x, z, xss);
+      sc[r] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the sentinels
       ix[r] = flat;
     } else {
       sc[r] = -1.0;
@@ -494,10 +495,10 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
     long long prev = -1;
     for (int base = 0; base < R && got < L.k_req; base += 32) {
       const int r = base + lane;
-      const long long slot = r < R ? L.cand_slot[ix[r]] : -1;
+      const long long slot = (r < R && ix[r] >= 0) ? L.cand_slot[ix[r]] : -1;
       const long long left = __shfl_up_sync(~0u, slot, 1);
       const long long before = lane == 0 ? prev : left;
-      const bool fresh = r < R && slot != before;
+      const bool fresh = slot >= 0 && slot != before;
       const unsigned fm = __ballot_sync(~0u, fresh);
       const int pos = got + __popc(fm & lanemask_lt());
       if (fresh && pos < L.k_req) s_slot[pos] = slot;

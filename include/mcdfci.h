@@ -179,6 +179,16 @@ int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* 
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
+/* Launch shape of the column kernel: CTAs per column, clusters of that size
+ * resident at once on this GPU, and entries per Hamiltonian column.  No
+ * counterpart in the reference (it has no GPU launch). */
+int mcd_debug_launch_info(mcd_solver* s, int32_t* cluster, int32_t* max_active_clusters, int32_t* entries_per_column);
+/* SM cycles spent in each phase of the leader kernel (16 phases: state load,
+ * finish, candidate slots, dedupe, refetch, sort, H_sub, update_x, publish,
+ * eig setup, tridiagonalisation, multisection, inverse iteration,
+ * back-transformation, Rayleigh quotient, eig finish), summed over launches
+ * since the previous call, which resets them.  No counterpart in the reference. */
+int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n);
 /* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);
 

@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "mcd_create", "mcd_create_from_fcidump", "mcd_destroy", "mcd_solve", "mcd_reset",
     "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
-    "mcd_debug_table_sums", "mcd_debug_picked",
+    "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_launch_info", "mcd_debug_leader_sections",
 )
 
 
@@ -130,6 +130,9 @@ def library() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
+    L.mcd_debug_leader_sections.argtypes = [vp, _u64p, ctypes.c_int32]
     _lib = L
     return L
 
@@ -384,6 +387,23 @@ class CDFCI:
         occ = ctypes.c_uint64()
         _check(library().mcd_debug_table_sums(self._h, xx, xz, ctypes.byref(occ)))
         return {"xx": tuple(xx), "xz": tuple(xz), "occupied": occ.value}
+
+    LEADER_SECTIONS = ("state", "finish", "cand_slots", "dedupe", "refetch", "sort", "hsub", "update_x",
+                       "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
+                       "rayleigh", "eig_finish")
+
+    def leader_sections(self) -> dict:
+        """SM cycles per leader-kernel phase since the previous call."""
+        import numpy as np
+
+        v = np.zeros(16, dtype=np.uint64)
+        _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), 16))
+        return {name: int(c) for name, c in zip(self.LEADER_SECTIONS, v)}
+
+    def launch_info(self) -> dict:
+        c, mac, e = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(library().mcd_debug_launch_info(self._h, ctypes.byref(c), ctypes.byref(mac), ctypes.byref(e)))
+        return {"cluster": c.value, "max_active_clusters": mac.value, "entries_per_column": e.value}
 
     def picked(self):
         import numpy as np

@@ -438,6 +438,25 @@ int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* oc
   });
 }
 
+int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n) {
+  return guarded([&] {
+    if (!s || !cycles) return fail(MCD_ERR_INVALID, "NULL argument.");
+    auto v = s->impl->leader_sections();
+    for (int32_t i = 0; i < n && i < static_cast<int32_t>(v.size()); ++i) cycles[i] = v[i];
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_launch_info(mcd_solver* s, int32_t* cluster, int32_t* max_active_clusters, int32_t* entries) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    if (cluster) *cluster = s->impl->cluster();
+    if (max_active_clusters) *max_active_clusters = s->impl->max_active_clusters();
+    if (entries) *entries = s->impl->entries_per_column();
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out) {
   return guarded([&] {
     if (!s || !k_out) return fail(MCD_ERR_INVALID, "NULL argument.");

@@ -215,130 +215,118 @@ __device__ __forceinline__ bool gen_entry(const HamDev& h, const Prelude& P, int
 }
 
 // ---------------------------------------------------------------------------
-// Warp-level top-m buffer.  Keys are the bit patterns of non-negative doubles,
-// so unsigned order is value order.
+// Per-warp top-M list of (key, slot) kept in registers, sorted descending:
+// element i is held by lane i % 32 in register i / 32.  Keys are the bit
+// pattern of the non-negative score plus one (so unsigned order is value
+// order); 0 marks an empty element.
+template <int R>
+struct TopList {
+  unsigned long long k[R];
+  unsigned p[R];
+};
 
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long w = __shfl_xor_sync(~0u, v, o);
-    v = w < v ? w : v;
+// Compare-exchange with lane ^ stride; this lane keeps the larger key if
+// keep_max.  Equal keys stay where they are on both sides.
+__device__ __forceinline__ void cmpx_lane(unsigned long long& k, unsigned& p, int stride, bool keep_max) {
+  const unsigned long long ok = __shfl_xor_sync(~0u, k, stride);
+  const unsigned op = __shfl_xor_sync(~0u, p, stride);
+  const bool take = keep_max ? (ok > k) : (ok < k);
+  if (take) {
+    k = ok;
+    p = op;
   }
-  return v;
 }
 
-// Keeps the m largest keys of buf[0..cnt) (equal keys: earlier positions
-// first), compacted in place.  Returns the new count and sets thr to the
-// smallest kept key.  cnt <= 5*32.
-__device__ int warp_keep_top(unsigned long long* key, long long* pay, int cnt, int m,
-                             unsigned long long& thr) {
+// Bitonic sort of one value per lane, ascending over lanes.
+__device__ __forceinline__ void sort32_ascending(unsigned long long& k, unsigned& p) {
   const int lane = threadIdx.x & 31;
-  const unsigned lt = lanemask_lt();
-  unsigned long long k[5];
-  long long pl[5];
-  bool ok[5];
 #pragma unroll
-  for (int j = 0; j < 5; ++j) {
-    const int idx = j * 32 + lane;
-    ok[j] = idx < cnt;
-    k[j] = ok[j] ? key[idx] : 0ull;
-    pl[j] = ok[j] ? pay[idx] : 0ll;
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const bool up = (lane & size) == 0;
+      const bool lower = (lane & stride) == 0;
+      cmpx_lane(k, p, stride, lower != up);
+    }
   }
-  __syncwarp();
-  unsigned long long K = 0;
-  bool exact = false;
-  for (int bit = 63; bit >= 0; --bit) {
-    const unsigned long long c = K | (1ull << bit);
-    unsigned n = 0;
+}
+
+// Sorts a bitonic list of M = 32R elements into descending order.
+template <int R>
+__device__ __forceinline__ void bitonic_merge_desc(TopList<R>& L) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int j = 0; j < 5; ++j) n += (ok[j] && k[j] >= c) ? 1u : 0u;
-    n = __reduce_add_sync(~0u, n);
-    if (n >= static_cast<unsigned>(m)) {
-      K = c;
-      if (n == static_cast<unsigned>(m)) {
-        exact = true;
-        break;
+  for (int sr = R / 2; sr > 0; sr >>= 1) {  // strides of 32*sr elements: across registers
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int jp = j ^ sr;
+      if (jp > j && L.k[jp] > L.k[j]) {
+        const unsigned long long tk = L.k[j];
+        const unsigned tp = L.p[j];
+        L.k[j] = L.k[jp];
+        L.p[j] = L.p[jp];
+        L.k[jp] = tk;
+        L.p[jp] = tp;
       }
     }
   }
-  bool keep[5];
-  if (exact) {
 #pragma unroll
-    for (int j = 0; j < 5; ++j) keep[j] = ok[j] && k[j] >= K;
-  } else {
-    unsigned ngt = 0;
+  for (int stride = 16; stride > 0; stride >>= 1) {
+    const bool lower = (lane & stride) == 0;
 #pragma unroll
-    for (int j = 0; j < 5; ++j) ngt += (ok[j] && k[j] > K) ? 1u : 0u;
-    ngt = __reduce_add_sync(~0u, ngt);
-    const int need = m - static_cast<int>(ngt);
-    int prior = 0;
-#pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      const bool eq = ok[j] && k[j] == K;
-      const unsigned em = __ballot_sync(~0u, eq);
-      const int rank = prior + __popc(em & lt);
-      keep[j] = (ok[j] && k[j] > K) || (eq && rank < need);
-      prior += __popc(em);
-    }
+    for (int j = 0; j < R; ++j) cmpx_lane(L.k[j], L.p[j], stride, lower);
   }
-  int pos = 0;
-  unsigned long long mn = ~0ull;
-#pragma unroll
-  for (int j = 0; j < 5; ++j) {
-    const unsigned km = __ballot_sync(~0u, keep[j]);
-    if (keep[j]) {
-      const int dst = pos + __popc(km & lt);
-      key[dst] = k[j];
-      pay[dst] = pl[j];
-      mn = k[j] < mn ? k[j] : mn;
-    }
-    pos += __popc(km);
-  }
-  thr = warp_min_u64(mn);
-  __syncwarp();
-  return pos;
 }
 
-struct WarpBuf {
-  unsigned long long* key;
-  long long* pay;
-  int cnt;
-  int m;
-  int cap;
-  bool have;               // thr valid
-  unsigned long long thr;  // keys <= thr are dropped
-};
-
-// Each lane offers one (key, payload) when `valid`.  Whole warp calls.
-__device__ __forceinline__ void warp_offer(WarpBuf& B, bool valid, unsigned long long k, long long p,
-                                           bool have_ext, unsigned long long thr_ext) {
-  bool have = B.have || have_ext;
-  unsigned long long thr = B.have ? B.thr : 0ull;
-  if (have_ext && (!B.have || thr_ext > thr)) thr = thr_ext;
-  bool pass = valid && (!have || k > thr);
-  unsigned bal = __ballot_sync(~0u, pass);
-  int n = __popc(bal);
-  if (B.cnt + n > B.cap) {
-    B.cnt = warp_keep_top(B.key, B.pay, B.cnt, B.m, B.thr);
-    B.have = true;
-    if (!have_ext || B.thr > thr_ext) thr = B.thr; else thr = thr_ext;
-    pass = valid && k > thr;
-    bal = __ballot_sync(~0u, pass);
-    n = __popc(bal);
+// Offers one (key, slot) per lane (key 0: nothing).  Keeps the list the
+// top M of everything offered so far.
+template <int R>
+__device__ __forceinline__ void toplist_offer(TopList<R>& L, unsigned long long key, unsigned slot) {
+  const unsigned long long theta = __shfl_sync(~0u, L.k[R - 1], 31);
+  if (!__any_sync(~0u, key > theta)) return;
+  sort32_ascending(key, slot);
+  // The top M of (descending list) u (ascending 32) is max(list[i], new[i - (M-32)]).
+  if (key > L.k[R - 1]) {
+    L.k[R - 1] = key;
+    L.p[R - 1] = slot;
   }
-  if (pass) {
-    const int dst = B.cnt + __popc(bal & lanemask_lt());
-    B.key[dst] = k;
-    B.pay[dst] = p;
-  }
-  B.cnt += n;
-  __syncwarp();
+  bitonic_merge_desc<R>(L);
 }
 
-__device__ __forceinline__ void warp_finish(WarpBuf& B) {
-  if (B.cnt > B.m) {
-    B.cnt = warp_keep_top(B.key, B.pay, B.cnt, B.m, B.thr);
-    B.have = true;
+// Merges another descending list, read from memory, into L.
+template <int R>
+__device__ __forceinline__ void toplist_merge(TopList<R>& L, const unsigned long long* ok, const unsigned* op) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    // Element i = 32j + lane pairs with the other list's element M-1-i.
+    const int i = (R - 1 - j) * 32 + (31 - lane);
+    const unsigned long long k2 = ok[i];
+    if (k2 > L.k[j]) {
+      L.k[j] = k2;
+      L.p[j] = op[i];
+    }
+  }
+  bitonic_merge_desc<R>(L);
+}
+
+template <int R>
+__device__ __forceinline__ void toplist_store(const TopList<R>& L, unsigned long long* k, unsigned* p) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    k[j * 32 + lane] = L.k[j];
+    p[j * 32 + lane] = L.p[j];
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void toplist_load(TopList<R>& L, const unsigned long long* k, const unsigned* p) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    L.k[j] = k[j * 32 + lane];
+    L.p[j] = p[j * 32 + lane];
   }
 }
 
@@ -350,7 +338,9 @@ __device__ __forceinline__ double score_of(double x, double z, dd xss) {
 
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kNT) column_kernel(ColumnLaunch L) {
+template <int R>
+__global__ void __launch_bounds__(kNT, 3) column_kernel(ColumnLaunch L) {
+  constexpr int M = 32 * R;
   cg::cluster_group cluster = cg::this_cluster();
   const int C = L.cluster;
   const int rank = static_cast<int>(cluster.block_rank());
@@ -359,45 +349,42 @@ __global__ void __launch_bounds__(kNT) column_kernel(ColumnLaunch L) {
   const int kcur = S->k_cur;
   if (col >= kcur) return;  // every CTA of this cluster has the same column
 
-  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ Prelude P;
+  __shared__ unsigned long long s_key[kW][M];
+  __shared__ unsigned s_pay[kW][M];
   __shared__ double w_newz[kW], w_dot[kW];
   __shared__ unsigned w_emit[kW], w_upd[kW], w_ins[kW];
-  __shared__ int w_cnt[kW];
-  __shared__ unsigned long long theta;  // cluster threshold + 1 (0: none yet), used in rank 0
   __shared__ double cta_newz, cta_dot;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned long long* keys0 = reinterpret_cast<unsigned long long*>(smem);
-  long long* pays0 = reinterpret_cast<long long*>(smem + static_cast<size_t>(kW) * L.cap_w * 8);
-
-  if (threadIdx.x == 0) theta = 0ull;
   if (warp == 0) build_prelude(P, S->det[col], L.ham.norb);
-  cluster.sync();
-  unsigned long long* theta0 = cluster.map_shared_rank(&theta, 0);
+  __syncthreads();
 
   const double dxc = S->dx[col];
   const double hd = S->hdiag[col];
   const dd xss = S->xss;
   const dd scale = S->scale;
   const dd zt{S->zt, 0.0};
-  const long long dslot = S->slot[col];
+  const unsigned dslot = static_cast<unsigned>(S->slot[col]);
   const int total = P.total;
   const int per = (total + C - 1) / C;
   const int beg = min(total, rank * per);
   const int end = min(total, beg + per);
   const int nrounds = (end - beg + kNT - 1) / kNT;
 
-  WarpBuf B{keys0 + warp * L.cap_w, pays0 + warp * L.cap_w, 0, L.m, L.cap_w, false, 0ull};
+  TopList<R> T;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    T.k[j] = 0ull;
+    T.p[j] = 0u;
+  }
   double acc_newz = 0.0, acc_dot = 0.0;
   unsigned emit = 0, upd = 0, ins = 0;
-  unsigned long long cthr = 0ull;
 
   for (int r = 0; r < nrounds; ++r) {
     const int e = beg + r * kNT + threadIdx.x;
-    bool cand = false;
     unsigned long long key = 0ull;
-    long long slot = -1;
+    unsigned slotu = 0u;
     if (e < end) {
       uint64_t a2, b2;
       double v;
@@ -405,6 +392,7 @@ __global__ void __launch_bounds__(kNT) column_kernel(ColumnLaunch L) {
         ++emit;
         const double dz = v * dxc;
         const bool above = dd_gt(dd_abs(dd_mul_d(scale, dz)), zt);
+        long long slot;
         if (e == 0) {
           slot = dslot;
         } else if (above) {
@@ -421,101 +409,107 @@ __global__ void __launch_bounds__(kNT) column_kernel(ColumnLaunch L) {
           ++upd;
           acc_newz += v * x;
           acc_dot += dz * x;
-          key = static_cast<unsigned long long>(__double_as_longlong(score_of(x, znew, xss)));
-          cand = true;
+          key = static_cast<unsigned long long>(__double_as_longlong(score_of(x, znew, xss))) + 1ull;
+          slotu = static_cast<unsigned>(slot);
         }
       }
     }
-    if ((r & 3) == 0) {
-      unsigned long long t = 0ull;
-      if (lane == 0) t = *reinterpret_cast<volatile unsigned long long*>(theta0);
-      cthr = __shfl_sync(~0u, t, 0);
-    }
-    const bool had = B.have;
-    const unsigned long long old = B.thr;
-    warp_offer(B, cand, key, slot, cthr != 0ull, cthr - 1ull);
-    if (B.have && (!had || B.thr != old) && lane == 0) atomicMax(theta0, B.thr + 1ull);
+    toplist_offer<R>(T, key, slotu);
   }
 
-  warp_finish(B);
   acc_newz = warp_sum(acc_newz);
   acc_dot = warp_sum(acc_dot);
   emit = __reduce_add_sync(~0u, emit);
   upd = __reduce_add_sync(~0u, upd);
   ins = __reduce_add_sync(~0u, ins);
+  toplist_store<R>(T, s_key[warp], s_pay[warp]);
   if (lane == 0) {
     w_newz[warp] = acc_newz;
     w_dot[warp] = acc_dot;
     w_emit[warp] = emit;
     w_upd[warp] = upd;
     w_ins[warp] = ins;
-    w_cnt[warp] = B.cnt;
   }
   __syncthreads();
-
-  if (warp == 0) {
-    for (int w = 1; w < kW; ++w) {
-      const int n = w_cnt[w];
-      const unsigned long long* k2 = keys0 + w * L.cap_w;
-      const long long* p2 = pays0 + w * L.cap_w;
-      for (int c0 = 0; c0 < n; c0 += 32) {
-        const int idx = c0 + lane;
-        const bool ok = idx < n;
-        warp_offer(B, ok, ok ? k2[idx] : 0ull, ok ? p2[idx] : -1ll, false, 0ull);
-      }
+  // Tree merge of the warp lists inside the CTA; the result lands in s_key[0].
+#pragma unroll
+  for (int half = kW / 2; half > 0; half >>= 1) {
+    if (warp < half) toplist_merge<R>(T, s_key[warp + half], s_pay[warp + half]);
+    __syncthreads();
+    if (warp < half) toplist_store<R>(T, s_key[warp], s_pay[warp]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double nz = 0.0, dt = 0.0;
+    unsigned long long e2 = 0, u2 = 0, i2 = 0;
+    for (int w = 0; w < kW; ++w) {
+      nz += w_newz[w];
+      dt += w_dot[w];
+      e2 += w_emit[w];
+      u2 += w_upd[w];
+      i2 += w_ins[w];
     }
-    warp_finish(B);
-    if (lane == 0) {
-      w_cnt[0] = B.cnt;
-      double nz = 0.0, dt = 0.0;
-      unsigned long long e2 = 0, u2 = 0, i2 = 0;
-      for (int w = 0; w < kW; ++w) {
-        nz += w_newz[w];
-        dt += w_dot[w];
-        e2 += w_emit[w];
-        u2 += w_upd[w];
-        i2 += w_ins[w];
-      }
-      cta_newz = nz;
-      cta_dot = dt;
-      if (e2) {
-        atomicAdd(&S->emitted, e2);
-        atomicAdd(&S->emitted_total, e2);
-      }
-      if (u2) {
-        atomicAdd(&S->updates, u2);
-        atomicAdd(&S->updates_total, u2);
-      }
-      if (i2) atomicAdd(&S->z_size, i2);
+    cta_newz = nz;
+    cta_dot = dt;
+    if (e2) {
+      atomicAdd(&S->emitted, e2);
+      atomicAdd(&S->emitted_total, e2);
     }
+    if (u2) {
+      atomicAdd(&S->updates, u2);
+      atomicAdd(&S->updates_total, u2);
+    }
+    if (i2) atomicAdd(&S->z_size, i2);
   }
   cluster.sync();
 
-  if (rank == 0 && warp == 0) {
-    for (int rr = 1; rr < C; ++rr) {
-      const int n = *cluster.map_shared_rank(&w_cnt[0], rr);
-      const unsigned long long* k2 = cluster.map_shared_rank(keys0, rr);
-      const long long* p2 = cluster.map_shared_rank(pays0, rr);
-      for (int c0 = 0; c0 < n; c0 += 32) {
-        const int idx = c0 + lane;
-        const bool ok = idx < n;
-        warp_offer(B, ok, ok ? k2[idx] : 0ull, ok ? p2[idx] : -1ll, false, 0ull);
-      }
+  if (rank == 0) {
+    // Warp w of CTA 0 merges the lists of CTAs w, w+kW (distributed shared memory).
+    TopList<R> U;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      U.k[j] = 0ull;
+      U.p[j] = 0u;
     }
-    warp_finish(B);
-    for (int j = lane; j < B.cnt; j += 32) {
-      L.cand_score[static_cast<size_t>(col) * L.m + j] = __longlong_as_double(static_cast<long long>(B.key[j]));
-      L.cand_slot[static_cast<size_t>(col) * L.m + j] = B.pay[j];
+    for (int rr = warp; rr < C; rr += kW) {
+      const unsigned long long* rk = cluster.map_shared_rank(&s_key[0][0], rr);
+      const unsigned* rp = cluster.map_shared_rank(&s_pay[0][0], rr);
+      toplist_merge<R>(U, rk, rp);
     }
-    if (lane == 0) {
-      double nz = 0.0, dt = 0.0;
-      for (int rr = 0; rr < C; ++rr) {
-        nz += *cluster.map_shared_rank(&cta_newz, rr);
-        dt += *cluster.map_shared_rank(&cta_dot, rr);
+    // Own CTA-list sits in s_key[0]; every warp is done reading it before
+    // s_key[w] is overwritten.
+    __syncthreads();
+    toplist_store<R>(U, s_key[warp], s_pay[warp]);
+    __syncthreads();
+#pragma unroll
+    for (int half = kW / 2; half > 0; half >>= 1) {
+      if (warp < half) toplist_merge<R>(U, s_key[warp + half], s_pay[warp + half]);
+      __syncthreads();
+      if (warp < half) toplist_store<R>(U, s_key[warp], s_pay[warp]);
+      __syncthreads();
+    }
+    if (warp == 0) {
+      int n = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int i = j * 32 + lane;
+        const bool ok = i < L.m && U.k[j] != 0ull;
+        if (ok) {
+          L.cand_score[static_cast<size_t>(col) * L.m + i] = __longlong_as_double(static_cast<long long>(U.k[j] - 1ull));
+          L.cand_slot[static_cast<size_t>(col) * L.m + i] = U.p[j];
+        }
+        n += __popc(__ballot_sync(~0u, ok));
       }
-      S->newz[col] = nz;
-      S->dot[col] = dt;
-      S->cand_n[col] = B.cnt;
+      if (lane == 0) {
+        double nz = 0.0, dt = 0.0;
+        for (int rr = 0; rr < C; ++rr) {
+          nz += *cluster.map_shared_rank(&cta_newz, rr);
+          dt += *cluster.map_shared_rank(&cta_dot, rr);
+        }
+        S->newz[col] = nz;
+        S->dot[col] = dt;
+        S->cand_n[col] = n;
+      }
     }
   }
   cluster.sync();
@@ -540,6 +534,48 @@ __global__ void __launch_bounds__(kNT) debug_column_kernel(HamDev h, Det d, doub
   }
 }
 
+template <int R>
+cudaLaunchConfig_t column_config(const ColumnLaunch& a, cudaStream_t s, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(a.k_grid * a.cluster, 1, 1);
+  cfg.blockDim = dim3(kNT, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = a.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <int R>
+cudaError_t launch_column_r(const ColumnLaunch& a, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(column_kernel<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = column_config<R>(a, s, attr);
+  return cudaLaunchKernelEx(&cfg, column_kernel<R>, a);
+}
+
+template <int R>
+int max_active_clusters_r(int cluster) {
+  ColumnLaunch a{};
+  a.k_grid = 64;
+  a.cluster = cluster;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = column_config<R>(a, 0, attr);
+  cudaFuncSetAttribute(column_kernel<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, column_kernel<R>, &cfg) != cudaSuccess) return -1;
+  return n;
+}
+
 }  // namespace
 
 int column_entries(int norb, int na, int nb) {
@@ -549,31 +585,16 @@ int column_entries(int norb, int na, int nb) {
   return t > 0x7fffffffLL ? -1 : static_cast<int>(t);
 }
 
-size_t column_smem_bytes(int m, int nthreads) {
-  const int cap = ((m + 31) / 32) * 32 + 32;
-  return static_cast<size_t>(nthreads / 32) * cap * 16;
+cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s) {
+  if (a.m <= 32) return launch_column_r<1>(a, s);
+  if (a.m <= 64) return launch_column_r<2>(a, s);
+  return launch_column_r<4>(a, s);
 }
 
-cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(column_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(a.k_grid * a.cluster, 1, 1);
-  cfg.blockDim = dim3(kNT, 1, 1);
-  cfg.dynamicSmemBytes = column_smem_bytes(a.m, kNT);
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = a.cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, column_kernel, a);
+int column_max_active_clusters(int cluster, int m) {
+  if (m <= 32) return max_active_clusters_r<1>(cluster);
+  if (m <= 64) return max_active_clusters_r<2>(cluster);
+  return max_active_clusters_r<4>(cluster);
 }
 
 cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,

@@ -177,6 +177,25 @@ __device__ __forceinline__ long long table_upsert(const TableDev& t, uint64_t a,
 }
 
 // ---------------------------------------------------------------------------
+// Section clock: thread 0 of a CTA adds the SM cycles since the previous mark
+// to acc[i].  Marks are placed right after block-wide barriers, so each entry
+// is the duration of one phase of the CTA.  acc may be null (no timing).
+struct SectionClock {
+  unsigned long long* acc;
+  long long t;
+  __device__ __forceinline__ void start() {
+    if (threadIdx.x == 0) t = clock64();
+  }
+  __device__ __forceinline__ void mark(int i) {
+    if (acc != nullptr && threadIdx.x == 0) {
+      const long long now = clock64();
+      atomicAdd(acc + i, static_cast<unsigned long long>(now - t));
+      t = now;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Warp helpers.
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;

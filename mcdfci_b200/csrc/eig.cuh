@@ -40,7 +40,7 @@ struct EigScratch {
 
 // Block-wide.  On return ws.y[0..n) holds an (unnormalised) eigenvector of the
 // lowest eigenvalue of the matrix originally in ws.A; ws.A is overwritten.
-__device__ void smallest_eigvec(EigScratch& ws, int n) {
+__device__ void smallest_eigvec(EigScratch& ws, int n, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int NT = blockDim.x;
   double* A = ws.A;
@@ -117,6 +117,8 @@ __device__ void smallest_eigvec(EigScratch& ws, int n) {
   }
   __syncthreads();
 
+  clk.mark(10);
+
   // 2. Multisection for the lowest eigenvalue of T.
   if (warp == 0) {
     double lo = 1e300, hi = -1e300, emax = 0.0;
@@ -171,25 +173,29 @@ __device__ void smallest_eigvec(EigScratch& ws, int n) {
     __syncthreads();
   }
 
+  clk.mark(11);
+
   // 3. Inverse iteration on T - sigma I (thread 0; u and l reuse hv and p).
   if (tid == 0) {
     const double sigma = ws.scal[2];
     const double tiny = 1e-290;
-    double* u = ws.hv;
+    double* ru = ws.hv;  // 1 / u_i
     double* l = ws.p;
-    u[0] = ws.d[0] - sigma;
-    if (fabs(u[0]) < tiny) u[0] = tiny;
+    double u = ws.d[0] - sigma;
+    if (fabs(u) < tiny) u = tiny;
+    ru[0] = 1.0 / u;
     for (int i = 1; i < n; ++i) {
-      l[i] = ws.e[i - 1] / u[i - 1];
-      u[i] = (ws.d[i] - sigma) - l[i] * ws.e[i - 1];
-      if (fabs(u[i]) < tiny) u[i] = tiny;
+      l[i] = ws.e[i - 1] * ru[i - 1];
+      u = (ws.d[i] - sigma) - l[i] * ws.e[i - 1];
+      if (fabs(u) < tiny) u = tiny;
+      ru[i] = 1.0 / u;
     }
     double* y = ws.y;
     for (int i = 0; i < n; ++i) y[i] = 1.0 + 0.0625 * static_cast<double>((7 * i + 3) % 11);
     for (int it = 0; it < 3; ++it) {
       for (int i = 1; i < n; ++i) y[i] -= l[i] * y[i - 1];
-      y[n - 1] /= u[n - 1];
-      for (int i = n - 2; i >= 0; --i) y[i] = (y[i] - ws.e[i] * y[i + 1]) / u[i];
+      y[n - 1] *= ru[n - 1];
+      for (int i = n - 2; i >= 0; --i) y[i] = (y[i] - ws.e[i] * y[i + 1]) * ru[i];
       double mx = 0.0;
       for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(y[i]));
       const double inv = mx > 0.0 ? 1.0 / mx : 1.0;
@@ -197,6 +203,8 @@ __device__ void smallest_eigvec(EigScratch& ws, int n) {
     }
   }
   __syncthreads();
+
+  clk.mark(12);
 
   // 4. Back-transformation y <- H_0 ... H_{n-3} y (warp 0).
   if (warp == 0) {

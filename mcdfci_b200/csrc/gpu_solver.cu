@@ -131,11 +131,6 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   entries_ = column_entries(ham_.norb, na_, nb_);
   if (entries_ < 0) throw McdError(MCD_ERR_UNSUPPORTED, "a Hamiltonian column has more than 2^31 entries.");
   n_words_ = 1 + (fci.norb - 1) / 64;
-  if (opt_.cluster > 0) {
-    cluster_ = opt_.cluster;
-  } else {
-    cluster_ = std::max(1, std::min(16, (entries_ + 1023) / 1024));
-  }
 
   // Table sizing as run_cdfci_wrapper (src/run_wrapper.h:203-213): the
   // largest power of two of determinants whose reference footprint
@@ -146,6 +141,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   pow2 /= 2;
   capacity_ = pow2;
   max_size_ = static_cast<unsigned long long>(0.79 * static_cast<double>(pow2));
+  if (capacity_ > (1ull << 32))
+    throw McdError(MCD_ERR_UNSUPPORTED, "max_memory asks for more than 2^32 hash slots (128 GB).");
 
   // Device.
   if (opt_.device >= 0) check(cudaSetDevice(opt_.device), "cudaSetDevice");
@@ -155,6 +152,18 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   } else {
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     own_stream_ = true;
+  }
+  // CTAs per column: the largest power of two up to 16 that still lets the
+  // clusters of all k columns be resident at once and leaves every CTA at
+  // least 256 column entries.
+  if (opt_.cluster > 0) {
+    cluster_ = opt_.cluster;
+  } else {
+    cluster_ = 1;
+    for (int c = 2; c <= 16; c *= 2) {
+      if (entries_ < c * 256 || column_max_active_clusters(c, opt_.m) < opt_.k) break;
+      cluster_ = c;
+    }
   }
 
   try {
@@ -203,10 +212,12 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
     d_state_ = device_alloc<IterState>(1, "iteration state");
     d_cand_score_ = device_alloc<double>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
-    d_cand_slot_ = device_alloc<long long>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
+    d_cand_slot_ = device_alloc<unsigned>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
     d_hsub_ = device_alloc<double>(static_cast<size_t>(kMaxK) * kMaxK, "H_sub");
     d_err_ = device_alloc<unsigned>(1, "error word");
     d_occ_ = device_alloc<unsigned long long>(1, "occupancy");
+    d_sect_ = device_alloc<unsigned long long>(kLeaderSections, "leader timers");
+    check(cudaMemsetAsync(d_sect_, 0, kLeaderSections * sizeof(unsigned long long), stream_), "memset");
   } catch (...) {
     release();
     throw;
@@ -224,7 +235,6 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   cl_.cand_score = d_cand_score_;
   cl_.cand_slot = d_cand_slot_;
   cl_.m = opt_.m;
-  cl_.cap_w = ((opt_.m + 31) / 32) * 32 + 32;
   cl_.cluster = cluster_;
   cl_.k_grid = opt_.k;
   cl_.na = na_;
@@ -236,6 +246,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.cand_score = d_cand_score_;
   ll_.cand_slot = d_cand_slot_;
   ll_.hsub_out = d_hsub_;
+  ll_.sect = d_sect_;
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
   check(cudaStreamSynchronize(stream_), "table upload");
@@ -255,6 +266,8 @@ void GpuSolver::release() {
   cudaFree(d_hsub_);
   cudaFree(d_err_);
   cudaFree(d_occ_);
+  cudaFree(d_sect_);
+  d_sect_ = nullptr;
   d_tables_ = nullptr;
   d_slots_ = nullptr;
   d_state_ = nullptr;
@@ -542,6 +555,14 @@ void GpuSolver::table_sums(dd* xx, dd* xz, unsigned long long* occupied) {
   *xx = a;
   *xz = b;
   *occupied = c;
+}
+
+std::vector<unsigned long long> GpuSolver::leader_sections() {
+  std::vector<unsigned long long> v(kLeaderSections);
+  check(cudaStreamSynchronize(stream_), "sync");
+  check(cudaMemcpy(v.data(), d_sect_, v.size() * 8, cudaMemcpyDeviceToHost), "copy");
+  check(cudaMemset(d_sect_, 0, v.size() * 8), "memset");
+  return v;
 }
 
 std::vector<std::pair<Det, double>> GpuSolver::picked() {

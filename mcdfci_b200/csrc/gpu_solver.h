@@ -69,12 +69,15 @@ class GpuSolver {
   std::vector<double> hsub(const std::vector<Det>& dets);
   void table_sums(dd* xx, dd* xz, unsigned long long* occupied);
   std::vector<std::pair<Det, double>> picked();
+  // Leader-kernel phase timers (SM cycles summed over launches since the last call).
+  std::vector<unsigned long long> leader_sections();
 
   const HamHost& ham() const { return ham_; }
   Det reference_det() const { return ref_; }
   long long table_capacity() const { return static_cast<long long>(capacity_); }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int cluster() const { return cluster_; }
+  int max_active_clusters() const { return column_max_active_clusters(cluster_, opt_.m); }
   int entries_per_column() const { return entries_; }
 
  private:
@@ -101,10 +104,11 @@ class GpuSolver {
   Slot* d_slots_ = nullptr;
   IterState* d_state_ = nullptr;
   double* d_cand_score_ = nullptr;
-  long long* d_cand_slot_ = nullptr;
+  unsigned* d_cand_slot_ = nullptr;
   double* d_hsub_ = nullptr;
   unsigned* d_err_ = nullptr;
   unsigned long long* d_occ_ = nullptr;
+  unsigned long long* d_sect_ = nullptr;
   HamDev hd_{};
   TableDev td_{};
   ColumnLaunch cl_{};

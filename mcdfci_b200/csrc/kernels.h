@@ -68,10 +68,9 @@ struct ColumnLaunch {
   HamDev ham;
   TableDev tab;
   IterState* st;
-  double* cand_score;     // [kMaxK][m]
-  long long* cand_slot;   // [kMaxK][m]
+  double* cand_score;     // [kMaxK][m] score of each column's candidates
+  unsigned* cand_slot;    // [kMaxK][m] their hash slots (tables have at most 2^32 slots)
   int m;
-  int cap_w;              // per-warp candidate buffer capacity (round_up(m,32)+32)
   int cluster;            // CTAs per column
   int k_grid;             // columns launched (>= k_cur)
   int na, nb;             // electrons per spin (fixed by the starting determinant)
@@ -82,14 +81,23 @@ struct LeaderLaunch {
   TableDev tab;
   IterState* st;
   const double* cand_score;
-  const long long* cand_slot;
+  const unsigned* cand_slot;
   double* hsub_out;       // [kMaxK*kMaxK] last H_sub (row-major, k_cur x k_cur)
+  unsigned long long* sect;  // [kLeaderSections] SM cycles per phase of the leader kernel, or null
   int m;
   int k_req;
 };
 
+// Phases of the leader kernel timed into LeaderLaunch::sect: 0 state load,
+// 1 finish + prefix, 2 candidate slots, 3 dedupe, 4 refetch, 5 sort, 6 H_sub,
+// 7 update_x, 8 publish, 9 eig setup, 10 tridiagonalisation, 11 multisection,
+// 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
+// 15 eig finish.
+constexpr int kLeaderSections = 16;
+
 // Launchers (column_kernel.cu / leader_kernel.cu).
-size_t column_smem_bytes(int m, int nthreads);
+// Clusters of `cluster` column CTAs that fit on the GPU at once.
+int column_max_active_clusters(int cluster, int m);
 int column_entries(int norb, int na, int nb);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);

@@ -142,8 +142,9 @@ __device__ __forceinline__ double score_of(double x, double z, dd xss) {
 }
 
 // ---------------------------------------------------------------------------
-// Eig update.  Inputs in shared memory: x[k], z[k]; H in global memory
-// (row-major k x k, symmetric).  Outputs dx[k] (shared), new xx / scale.
+// Eig update.  Inputs x[k], z[k] in shared memory; H (row-major k x k,
+// symmetric) in shared or global memory; `work` is shared scratch of
+// eig_work_doubles(k) doubles.  Outputs dx[k] (shared), new xx and scale.
 
 struct EigResult {
   dd xx, scale;
@@ -152,21 +153,26 @@ struct EigResult {
   double resid;
 };
 
-__device__ EigResult eig_update(const double* Hg, int k, const double* x, const double* z, dd xx, dd xz,
-                                double* dx, double* smem_d) {
+__host__ __device__ constexpr size_t eig_work_doubles(int k) {
+  return static_cast<size_t>(k + 1) * (k + 1) + 12 * static_cast<size_t>(k + 1) + 64;
+}
+
+__device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
+                                double* dx, double* work, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1;
   __shared__ dd s_red[32];
   __shared__ double s_redd[32];
   __shared__ int s_branch;
   __shared__ int s_ibest;
+  __shared__ dd s_rq;
   EigResult res;
 
   // x'x, x'z, Hx, x'Hx in double-double, rounded where the reference works in double.
-  double* Hx = smem_d;  // [k]
+  double* Hx = work;  // [k]
   for (int r = warp; r < k; r += 32) {
     dd s{0.0, 0.0};
-    for (int c = lane; c < k; c += 32) s = dd_add(s, dd_two_prod(Hg[r * k + c], x[c]));
+    for (int c = lane; c < k; c += 32) s = dd_add(s, dd_two_prod(H[r * k + c], x[c]));
     s = warp_sum_dd(s);
     if (lane == 0) Hx[r] = dd_to_d(s);
   }
@@ -199,8 +205,7 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
   const int off = branch == 1 ? 1 : 0;
   const double y1 = s_y1;
 
-  // Scratch layout after Hx (k doubles).
-  double* base = smem_d + ((k + 1) & ~1) + 2;
+  double* base = work + ((k + 1) & ~1) + 2;
   EigScratch ws;
   ws.lda = n;
   ws.A = base;
@@ -218,13 +223,14 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
   ws.scal = ws.part + 32;    // [8]
   ws.ibest = &s_ibest;
 
-  // Build B.
+  // B = [[b00, b'], [b, H]] with b = (z - Hx) / y1; only the upper triangle of
+  // H is used, as dsyevr with UPLO='L' on the row-major array does.
   for (int idx = tid; idx < n * n; idx += blockDim.x) {
     const int r = idx / n, c = idx - r * n;
     double v;
     if (r >= off && c >= off) {
       const int i = r - off, j = c - off;
-      v = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];  // upper triangle, as dsyevr UPLO='L' column-major
+      v = (i <= j) ? H[i * k + j] : H[j * k + i];
     } else if (r == 0 && c == 0) {
       v = s_b00;
     } else {
@@ -235,8 +241,10 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
     if (r == 0) bvec[c] = v;
   }
   __syncthreads();
+  clk.mark(9);
 
-  smallest_eigvec(ws, n);
+  smallest_eigvec(ws, n, clk);
+  clk.mark(13);
 
   // Normalise in double-double; fix the sign.
   if (warp == 0) {
@@ -260,29 +268,32 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
   }
   __syncthreads();
 
-  // Rayleigh quotient v'Bv in double-double.
+  // Rayleigh quotient v'Bv in double-double, and B v in double for the residual.
   {
     dd acc{0, 0};
     for (int r = warp; r < n; r += 32) {
       dd s{0, 0};
+      double sd = 0.0;
       for (int c = lane; c < n; c += 32) {
         double brc;
         if (r >= off && c >= off) {
           const int i = r - off, j = c - off;
-          brc = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];
+          brc = (i <= j) ? H[i * k + j] : H[j * k + i];
         } else {
           brc = bvec[r == 0 ? c : r];
         }
         s = dd_add(s, dd_mul_d(dd{vhi[c], vlo[c]}, brc));
+        sd += brc * vhi[c];
       }
       s = warp_sum_dd(s);
       s = dd{__shfl_sync(~0u, s.hi, 0), __shfl_sync(~0u, s.lo, 0)};
+      sd = __shfl_sync(~0u, warp_sum(sd), 0);
       acc = dd_add(acc, dd_mul(s, dd{vhi[r], vlo[r]}));
+      if (lane == 0) ws.hv[r] = sd;  // (B v)_r for the residual
     }
     if (lane == 0) s_red[warp] = acc;
   }
   __syncthreads();
-  __shared__ dd s_rq;
   if (tid == 0) {
     dd t{0, 0};
     for (int w = 0; w < 32; ++w) t = dd_add(t, s_red[w]);
@@ -291,35 +302,24 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
   __syncthreads();
   const dd rq = s_rq;
   const double lam = dd_to_d(rq);
-  // Residual ||B v - lambda v|| (diagnostic, reported like the reference's max residual).
-  {
+  if (warp == 0) {
     double acc = 0.0;
-    for (int r = warp; r < n; r += 32) {
-      double s = 0.0;
-      for (int c = lane; c < n; c += 32) {
-        double brc;
-        if (r >= off && c >= off) {
-          const int i = r - off, j = c - off;
-          brc = (i <= j) ? Hg[i * k + j] : Hg[j * k + i];
-        } else {
-          brc = bvec[r == 0 ? c : r];
-        }
-        s += brc * vhi[c];
-      }
-      s = warp_sum(s);
-      const double t = s - lam * vhi[r];
+    for (int r = lane; r < n; r += 32) {
+      const double t = ws.hv[r] - lam * vhi[r];
       acc += t * t;
     }
-    if (lane == 0) s_redd[warp] = acc;
+    acc = warp_sum(acc);
+    if (lane == 0) s_redd[0] = acc;
   }
   __syncthreads();
-  double rr = 0.0;
-  for (int w = 0; w < 32; ++w) rr += s_redd[w];
-  res.resid = sqrt(rr);
+  clk.mark(14);
+  res.resid = sqrt(s_redd[0]);
   res.branch = branch;
   res.ok = true;
 
   if (branch == 1) {
+    // lambda_q = -rq, gamma = v0 / y1, scale = gamma sqrt(lambda_q),
+    // xx = lambda_q / scale^2, dx_i = v_{i+1} / gamma - x_i (src/solver.h:516-538).
     const dd lq = dd_neg(rq);
     const dd v0{vhi[0], vlo[0]};
     const dd gamma = dd_div_d(v0, y1);
@@ -332,6 +332,7 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
       dx[i] = dd_to_d(dd_add_d(q, -x[i]));
     }
   } else {
+    // First iteration: xx = -lambda, scale = 1, dx = v sqrt(-lambda) - x (src/solver.h:552-598).
     res.ok = lam < 0.0 && isfinite(lam);
     const double sq = sqrt(-lam);
     res.xx = dd{-lam, 0.0};
@@ -348,9 +349,10 @@ __device__ EigResult eig_update(const double* Hg, int k, const double* x, const 
 // ---------------------------------------------------------------------------
 
 // End of iteration t (src/wavefunction.h:557-565,583): z[D_c] = new_z_c for
-// the picked determinants, then xz += sum_c dot_c.  Block-wide.
-__device__ void finish_iteration(IterState* S, const TableDev& T, bool pending) {
-  if (!pending) return;
+// the picked determinants, then xz += sum_c dot_c.  Block-wide, on a state
+// copy `S` (shared or global); table stores go to global memory.
+__device__ void finish_iteration(IterState* S, const TableDev& T) {
+  if (!S->pending) return;
   const int k = S->k_cur;
   if (static_cast<int>(threadIdx.x) < k) {
     Slot* sp = T.slots + S->slot[threadIdx.x];
@@ -364,42 +366,90 @@ __device__ void finish_iteration(IterState* S, const TableDev& T, bool pending) 
     S->xz = xz;
     S->pending = 0;
   }
+  __syncthreads();
 }
 
-__global__ void finish_kernel(LeaderLaunch L) {
-  finish_iteration(L.st, L.tab, L.st->pending != 0);
+__global__ void finish_kernel(LeaderLaunch L) { finish_iteration(L.st, L.tab); }
+
+__device__ __forceinline__ unsigned hash32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
 }
+
+// Block-wide exclusive position of a kept element within one chunk of
+// blockDim.x elements; returns the chunk's kept count through *chunk_total.
+__device__ __forceinline__ int block_rank(bool keep, int* wsum, int* chunk_total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(~0u, keep);
+  if (lane == 0) wsum[warp] = __popc(b);
+  __syncthreads();
+  if (warp == 0) {
+    const int v = lane < static_cast<int>(blockDim.x >> 5) ? wsum[lane] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(~0u, incl, o);
+      if (lane >= o) incl += t;
+    }
+    wsum[lane] = incl - v;  // exclusive
+    if (lane == 31) wsum[32] = incl;
+  }
+  __syncthreads();
+  const int pos = wsum[warp] + __popc(b & lanemask_lt());
+  *chunk_total = wsum[32];
+  __syncthreads();
+  return pos;
+}
+
+constexpr unsigned kNoSlot = 0xFFFFFFFFu;
 
 __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(16) IterState sS;
   __shared__ int s_off[kMaxK + 1];
-  __shared__ int s_k, s_R;
+  __shared__ int s_wsum[33];
+  __shared__ int s_R, s_U;
   __shared__ unsigned s_err;
-  __shared__ long long s_slot[kMaxK];
+  __shared__ unsigned s_slot[kMaxK];
   __shared__ Det s_det[kMaxK];
   __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
   __shared__ unsigned char s_occ[32][128];
   __shared__ unsigned long long s_newx;
 
-  IterState* S = L.st;
+  IterState* G = L.st;
   const TableDev& T = L.tab;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m = L.m;
+  SectionClock clk{L.sect, 0};
+  clk.start();
 
-  // 1. Finish the previous iteration (unless finish_kernel already did).
-  const int kprev = S->k_cur;
-  const bool pending = S->pending != 0;
-  finish_iteration(S, T, pending);
+  // 0. Iteration state into shared memory.
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(G);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sS);
+    for (int i = tid; i < static_cast<int>(sizeof(IterState) / 8); i += kLT) dst[i] = src[i];
+  }
   if (tid == 0) {
-    if (*T.n_occupied > S->occupancy_limit) atomicOr(T.err, kErrOverflow);
     s_err = *reinterpret_cast<volatile unsigned*>(T.err);
+    if (*T.n_occupied > L.st->occupancy_limit) {
+      atomicOr(T.err, kErrOverflow);
+      s_err |= kErrOverflow;
+    }
     s_newx = 0;
   }
+  __syncthreads();
+  clk.mark(0);
+
+  // 1. Finish the previous iteration (unless finish_kernel already did).
+  const int kprev = sS.k_cur;
+  finish_iteration(&sS, T);
   if (warp == 0) {
-    // Exclusive prefix of the candidate counts over the columns.
     int run = 0;
     for (int base = 0; base < kMaxK; base += 32) {
-      const int cc = (base + lane < kprev) ? S->cand_n[base + lane] : 0;
+      const int cc = (base + lane < kprev) ? sS.cand_n[base + lane] : 0;
       int incl = cc;
       for (int o = 1; o < 32; o <<= 1) {
         const int t = __shfl_up_sync(~0u, incl, o);
@@ -414,60 +464,101 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
     }
   }
   __syncthreads();
+  clk.mark(1);
   if (s_err != 0u || s_R == 0) {
     if (tid == 0) {
       if (s_R == 0 && s_err == 0u) atomicOr(T.err, kErrCandidates);
-      S->k_cur = 0;
+      G->xz = sS.xz;
+      G->pending = 0;
+      G->k_cur = 0;
     }
     return;
   }
 
-  // 2. Refetch the candidates and score them.
+  // 2. Candidate slots; duplicates (one determinant in several columns) removed
+  //    with a shared-memory hash set.
   const int R = s_R;
-  int P = 1;
-  while (P < R) P <<= 1;
-  double* sc = reinterpret_cast<double*>(smem);
-  int* ix = reinterpret_cast<int*>(sc + P);
-  const dd xss = S->xss;
-  for (int r = tid; r < P; r += kLT) {
-    if (r < R) {
-      int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_off[mid] <= r) lo = mid; else hi = mid;
+  int PR = 2;  // >= 2 keeps the score array (which reuses the hash set) 8-byte aligned
+  while (PR < R) PR <<= 1;
+  unsigned* us = reinterpret_cast<unsigned*>(smem);          // [PR] slots, compacted in place
+  unsigned* hs = us + PR;                                     // [2*PR] hash set; later scores (double[PR])
+  const int H = 2 * PR;
+  for (int i = tid; i < H; i += kLT) hs[i] = kNoSlot;
+  for (int r = tid; r < R; r += kLT) {
+    int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_off[mid] <= r) lo = mid; else hi = mid;
+    }
+    us[r] = L.cand_slot[lo * m + (r - s_off[lo])];
+  }
+  __syncthreads();
+  clk.mark(2);
+  {
+    int total = 0;
+    for (int base = 0; base < R; base += kLT) {
+      const int r = base + tid;
+      const unsigned s = r < R ? us[r] : kNoSlot;
+      bool keep = false;
+      if (r < R) {
+        unsigned h = hash32(s) & static_cast<unsigned>(H - 1);
+        for (int probe = 0; probe < H; ++probe) {
+          const unsigned old = atomicCAS(&hs[h], kNoSlot, s);
+          if (old == kNoSlot) {
+            keep = true;
+            break;
+          }
+          if (old == s) break;
+          h = (h + 1) & static_cast<unsigned>(H - 1);
+        }
       }
-      const int j = r - s_off[lo];
-      const int flat = lo * m + j;
-      const long long slot = L.cand_slot[flat];
-      const Slot* sp = T.slots + slot;
+      int chunk = 0;
+      const int pos = block_rank(keep, s_wsum, &chunk);
+      if (keep) us[total + pos] = s;
+      total += chunk;
+      __syncthreads();
+    }
+    if (tid == 0) s_U = total;
+  }
+  __syncthreads();
+  clk.mark(3);
+  const int U = s_U;
+  int P = 1;
+  while (P < U) P <<= 1;
+
+  // 3. Scores of the unique candidates from the table (refetch).
+  double* sc = reinterpret_cast<double*>(hs);  // [P]
+  const dd xss = sS.xss;
+  for (int u = tid; u < P; u += kLT) {
+    if (u < U) {
+      const Slot* sp = T.slots + us[u];
       const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
       const double g = score_of(x, z, xss);
-      sc[r] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the sentinels
-      ix[r] = flat;
+      sc[u] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the padding
     } else {
-      sc[r] = -1.0;
-      ix[r] = -1;
+      sc[u] = -1.0;
+      us[u] = kNoSlot;
     }
   }
   __syncthreads();
+  clk.mark(4);
 
-  // 3. Bitonic sort, highest priority first: larger score, then the larger
-  //    determinant in the reference order.
-  const int nwords = S->n_words;
+  // 4. Bitonic sort, highest priority first: larger score, then the larger
+  //    determinant in the reference order (ties between different
+  //    determinants read their keys from the table).
+  const int nwords = sS.n_words;
   for (int size = 2; size <= P; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       for (int t = tid; t < (P >> 1); t += kLT) {
         const int i = 2 * stride * (t / stride) + (t % stride);
         const int j = i + stride;
         const double si = sc[i], sj = sc[j];
-        bool jfirst;  // j has higher priority than i
+        bool jfirst;
         if (si != sj) {
           jfirst = sj > si;
-        } else if (ix[i] < 0 || ix[j] < 0) {
-          jfirst = false;
         } else {
-          const long long a = L.cand_slot[ix[i]], b = L.cand_slot[ix[j]];
-          if (a == b) {
+          const unsigned a = us[i], b = us[j];
+          if (a == kNoSlot || b == kNoSlot || a == b) {
             jfirst = false;
           } else {
             uint64_t ia, ib, ja, jb;
@@ -480,73 +571,65 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
         if (jfirst == up) {
           sc[i] = sj;
           sc[j] = si;
-          const int tmp = ix[i];
-          ix[i] = ix[j];
-          ix[j] = tmp;
+          const unsigned tmp = us[i];
+          us[i] = us[j];
+          us[j] = tmp;
         }
       }
       __syncthreads();
     }
   }
-
-  // 4. First k distinct determinants (duplicates are adjacent).
-  if (warp == 0) {
-    int got = 0;
-    long long prev = -1;
-    for (int base = 0; base < R && got < L.k_req; base += 32) {
-      const int r = base + lane;
-      const long long slot = (r < R && ix[r] >= 0) ? L.cand_slot[ix[r]] : -1;
-      const long long left = __shfl_up_sync(~0u, slot, 1);
-      const long long before = lane == 0 ? prev : left;
-      const bool fresh = slot >= 0 && slot != before;
-      const unsigned fm = __ballot_sync(~0u, fresh);
-      const int pos = got + __popc(fm & lanemask_lt());
-      if (fresh && pos < L.k_req) s_slot[pos] = slot;
-      got += __popc(fm);
-      prev = __shfl_sync(~0u, slot, 31);
-    }
-    if (lane == 0) s_k = got < L.k_req ? got : L.k_req;
-  }
-  __syncthreads();
-  const int k = s_k;
+  clk.mark(5);
+  const int k = U < L.k_req ? U : L.k_req;
   if (tid < k) {
-    const Slot* sp = T.slots + s_slot[tid];
+    const unsigned slot = us[tid];
+    const Slot* sp = T.slots + slot;
     uint64_t a, b;
     load_key(sp, a, b);
+    s_slot[tid] = slot;
     s_det[tid] = Det{a, b};
     s_x[tid] = load_relaxed(&sp->x);
     s_z[tid] = load_relaxed(&sp->z);
   }
   __syncthreads();
 
-  // 5. H_sub.
-  double* Hg = L.hsub_out;
+  // 5. H_sub: in shared memory when it fits beside the eig scratch, else in
+  //    the global copy (which is written either way for inspection).
+  const bool h_in_smem = k <= 64;
+  double* Hs = h_in_smem ? reinterpret_cast<double*>(smem) : L.hsub_out;
+  double* work = h_in_smem ? Hs + k * k : reinterpret_cast<double*>(smem);
   for (int t = tid; t < k * k; t += kLT) {
     const int i = t / k, j = t - i * k;
     if (i < j) {
       const double v = off_diagonal(L.ham, s_det[i], s_det[j]);
-      Hg[i * k + j] = v;
-      Hg[j * k + i] = v;
+      Hs[i * k + j] = v;
+      Hs[j * k + i] = v;
     }
   }
   for (int i = warp; i < k; i += 32) {
     const double v = diagonal_warp(L.ham, s_det[i], s_occ[warp]);
-    if (lane == 0) Hg[i * k + i] = v;
+    if (lane == 0) Hs[i * k + i] = v;
   }
   __threadfence_block();
   __syncthreads();
+  clk.mark(6);
+  if (h_in_smem)
+    for (int t = tid; t < k * k; t += kLT) L.hsub_out[t] = Hs[t];
 
   // 6. Eig update.
-  const EigResult er = eig_update(Hg, k, s_x, s_z, S->xx, S->xz, s_dx, reinterpret_cast<double*>(smem));
+  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk);
+  clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {
       atomicOr(T.err, kErrEig);
-      S->k_cur = 0;
+      G->xz = sS.xz;
+      G->pending = 0;
+      G->k_cur = 0;
     }
     return;
   }
 
-  // 7. update_x.
+  // 7. update_x: x[D_i] += dx_i; xz += z_i dx_i; x_size counts dets whose x was 0.
   if (tid < k) {
     Slot* sp = T.slots + s_slot[tid];
     const double x0 = s_x[tid];
@@ -554,34 +637,38 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
     if (x0 == 0.0) atomicAdd(&s_newx, 1ull);
   }
   __syncthreads();
+  clk.mark(7);
+
+  // 8. Publish the next iteration.
   if (tid == 0) {
-    dd xz = S->xz;
+    dd xz = sS.xz;
     double mx = 0.0;
     for (int i = 0; i < k; ++i) {
       xz = dd_add_d(xz, s_z[i] * s_dx[i]);
       mx = fmax(mx, fabs(s_dx[i]));
     }
-    S->xz = xz;
-    S->xx = er.xx;
-    S->scale = er.scale;
-    S->xss = dd_mul(er.xx, dd_mul(er.scale, er.scale));
-    S->x_size += s_newx;
-    S->dx_max = mx;
-    S->eig_residual_max = fmax(S->eig_residual_max, er.resid);
-    S->last_branch = er.branch;
-    S->emitted = 0;
-    S->updates = 0;
-    S->iter += 1;
-    S->k_cur = k;
-    S->pending = 1;
+    G->xz = xz;
+    G->xx = er.xx;
+    G->scale = er.scale;
+    G->xss = dd_mul(er.xx, dd_mul(er.scale, er.scale));
+    G->x_size = sS.x_size + s_newx;
+    G->dx_max = mx;
+    G->eig_residual_max = fmax(sS.eig_residual_max, er.resid);
+    G->last_branch = er.branch;
+    G->emitted = 0;
+    G->updates = 0;
+    G->iter = sS.iter + 1;
+    G->k_cur = k;
+    G->pending = 1;
   }
-  // 8. Publish.
   if (tid < k) {
-    S->det[tid] = s_det[tid];
-    S->slot[tid] = s_slot[tid];
-    S->dx[tid] = s_dx[tid];
-    S->hdiag[tid] = Hg[tid * k + tid];
+    G->det[tid] = s_det[tid];
+    G->slot[tid] = s_slot[tid];
+    G->dx[tid] = s_dx[tid];
+    G->hdiag[tid] = Hs[tid * k + tid];
   }
+  __syncthreads();
+  clk.mark(8);
 }
 
 // Initial state (CDFCI::solve, src/solver.h:862-873): x = e_ref, z = H[:,ref]
@@ -640,7 +727,8 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, const double* 
     s_z[i] = z[i];
   }
   __syncthreads();
-  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem));
+  SectionClock clk{nullptr, 0};
+  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
   for (int i = threadIdx.x; i < k; i += blockDim.x) dx[i] = s_dx[i];
   if (threadIdx.x == 0) {
     out[0] = er.xx;
@@ -653,11 +741,11 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, const double* 
 }  // namespace
 
 size_t leader_smem_bytes(int k, int m) {
-  size_t P = 1;
+  size_t P = 2;
   while (P < static_cast<size_t>(k) * m) P <<= 1;
-  const size_t pick = P * (sizeof(double) + sizeof(int));
-  const size_t n = static_cast<size_t>(k) + 1;
-  const size_t eig = (n * n + 12 * n + 128) * sizeof(double);
+  const size_t pick = P * 4 + 2 * P * 4;  // slots + hash set (the hash set area later holds P doubles)
+  const size_t hs = (k <= 64 ? static_cast<size_t>(k) * k : 0) * sizeof(double);
+  const size_t eig = hs + eig_work_doubles(k) * sizeof(double);
   return pick > eig ? pick : eig;
 }
 
@@ -691,7 +779,7 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
 
 cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
                       double* dx, dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
-  const size_t bytes = leader_smem_bytes(k, 1);
+  const size_t bytes = eig_work_doubles(k) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(debug_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(bytes));
   if (e != cudaSuccess) return e;

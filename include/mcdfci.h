@@ -78,7 +78,7 @@ typedef struct mcd_options {
   int32_t n_ref_det_occ;
   int32_t coordinate_pick;     /* MCD_PICK_GCD_GRAD */
   int32_t coordinate_update;   /* MCD_UPDATE_EIG (the reference's default, "ls", is unsupported) */
-  int32_t cluster;             /* CTAs per Hamiltonian column, 1..16; 0 = chosen from the column length */
+  int32_t groups;              /* CTAs per Hamiltonian column; 0 = chosen from the column length */
   int32_t verbose;             /* 1: print the reference's report table to stdout */
   void* stream;                /* cudaStream_t to run on; NULL = a stream owned by the solver */
   int32_t device;              /* CUDA device ordinal; -1 = the current device */
@@ -179,12 +179,12 @@ int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* 
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
-/* Launch shape of the column kernel: CTAs per column, clusters of that size
- * resident at once on this GPU, and entries per Hamiltonian column.  No
- * counterpart in the reference (it has no GPU launch). */
-int mcd_debug_launch_info(mcd_solver* s, int32_t* cluster, int32_t* max_active_clusters, int32_t* entries_per_column);
+/* Launch shape of the column kernel: CTAs per column, length of the per-CTA
+ * candidate lists, and entries per Hamiltonian column.  No counterpart in the
+ * reference (it has no GPU launch). */
+int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, int32_t* entries_per_column);
 /* SM cycles spent in each phase of the leader kernel (16 phases: state load,
- * finish, candidate slots, dedupe, refetch, sort, H_sub, update_x, publish,
+ * finish, candidate gather, top-k, tie sort, picked, H_sub, update_x, publish,
  * eig setup, tridiagonalisation, multisection, inverse iteration,
  * back-transformation, Rayleigh quotient, eig finish), summed over launches
  * since the previous call, which resets them.  No counterpart in the reference. */

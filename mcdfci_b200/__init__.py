@@ -67,7 +67,7 @@ class mcd_options(ctypes.Structure):
         ("max_memory", ctypes.c_double), ("threshold", ctypes.c_double),
         ("ref_det_occ", ctypes.POINTER(ctypes.c_int32)), ("n_ref_det_occ", ctypes.c_int32),
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
-        ("cluster", ctypes.c_int32), ("verbose", ctypes.c_int32),
+        ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32),
     ]
 
@@ -251,7 +251,7 @@ def make_options(**kw) -> mcd_options:
     """mcd_options with the reference defaults, then keyword overrides
     (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
     z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
-    ("eig"|"ls"), cluster, verbose, stream, device)."""
+    ("eig"|"ls"), groups, verbose, stream, device)."""
     o = mcd_options()
     library().mcd_options_default(ctypes.byref(o))
     occ = kw.pop("ref_det_occ", None)
@@ -388,7 +388,7 @@ class CDFCI:
         _check(library().mcd_debug_table_sums(self._h, xx, xz, ctypes.byref(occ)))
         return {"xx": tuple(xx), "xz": tuple(xz), "occupied": occ.value}
 
-    LEADER_SECTIONS = ("state", "finish", "cand_slots", "dedupe", "refetch", "sort", "hsub", "update_x",
+    LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
                        "rayleigh", "eig_finish")
 
@@ -403,7 +403,7 @@ class CDFCI:
     def launch_info(self) -> dict:
         c, mac, e = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _check(library().mcd_debug_launch_info(self._h, ctypes.byref(c), ctypes.byref(mac), ctypes.byref(e)))
-        return {"cluster": c.value, "max_active_clusters": mac.value, "entries_per_column": e.value}
+        return {"groups": c.value, "list_size": mac.value, "entries_per_column": e.value}
 
     def picked(self):
         import numpy as np

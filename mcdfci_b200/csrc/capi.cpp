@@ -63,7 +63,7 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   if (o->ref_det_occ && o->n_ref_det_occ > 0) s.ref_det_occ.assign(o->ref_det_occ, o->ref_det_occ + o->n_ref_det_occ);
   s.coordinate_pick = o->coordinate_pick;
   s.coordinate_update = o->coordinate_update;
-  s.cluster = o->cluster;
+  s.groups = o->groups;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -145,7 +145,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   o->z_threshold_search = cd.at("z_threshold_search").as_bool("z_threshold_search") ? 1 : 0;
   o->max_memory = cd.at("max_memory").as_number("max_memory");
   o->threshold = option.at("hamiltonian").at("threshold").as_number("hamiltonian:threshold");
-  if (cd.has("cluster")) o->cluster = static_cast<int32_t>(cd.at("cluster").as_number("cluster"));
+  if (cd.has("groups")) o->groups = static_cast<int32_t>(cd.at("groups").as_number("groups"));
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -179,7 +179,7 @@ void mcd_options_default(mcd_options* o) {
   o->threshold = 1e-13;
   o->coordinate_pick = MCD_PICK_GCD_GRAD;
   o->coordinate_update = MCD_UPDATE_EIG;
-  o->cluster = 0;
+  o->groups = 0;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;
@@ -339,7 +339,7 @@ int mcd_run_json(const char* input_json_path) {
               << std::fixed << std::setprecision(3) << s->impl->table_capacity() * 32.0 / 1073741824.0
               << " GB) and can store " << s->impl->max_wavefunction_size() << " determinants at most." << std::endl;
     std::cout << "Each Hamiltonian column has " << s->impl->entries_per_column() << " candidate entries, "
-              << s->impl->cluster() << " CTA(s) per column." << std::endl
+              << s->impl->groups() << " CTA(s) per column." << std::endl
               << std::endl;
     rc = mcd_solve(s, nullptr, nullptr);
     const std::string err = g_last_error;
@@ -447,11 +447,11 @@ int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n) {
   });
 }
 
-int mcd_debug_launch_info(mcd_solver* s, int32_t* cluster, int32_t* max_active_clusters, int32_t* entries) {
+int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, int32_t* entries) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
-    if (cluster) *cluster = s->impl->cluster();
-    if (max_active_clusters) *max_active_clusters = s->impl->max_active_clusters();
+    if (groups) *groups = s->impl->groups();
+    if (list_size) *list_size = s->impl->list_size();
     if (entries) *entries = s->impl->entries_per_column();
     return MCD_OK;
   });

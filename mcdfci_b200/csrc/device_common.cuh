@@ -136,12 +136,13 @@ __device__ __forceinline__ double load_relaxed(const double* p) {
   return v;
 }
 
-// Linear probing.  Returns the slot index of (a,b) or -1 if absent.
-__device__ __forceinline__ long long table_find(const TableDev& t, uint64_t a, uint64_t b) {
-  uint64_t i = det_hash(a, b) & t.mask;
+// Linear probing, continuing from the home slot i whose key (ka, kb) the
+// caller has already loaded (so that the first probe can be in flight while
+// the caller does other work).  Returns the slot index of (a,b) or -1 if absent.
+__device__ __forceinline__ long long table_find_from(const TableDev& t, uint64_t a, uint64_t b, uint64_t i,
+                                                     uint64_t ka, uint64_t kb) {
   for (int p = 0; p < t.max_probe; ++p) {
-    uint64_t ka, kb;
-    load_key(t.slots + i, ka, kb);
+    if (p > 0) load_key(t.slots + i, ka, kb);
     if (ka == a && kb == b) return static_cast<long long>(i);
     if (ka == kEmptyKey && kb == kEmptyKey) return -1;
     i = (i + 1) & t.mask;
@@ -150,15 +151,22 @@ __device__ __forceinline__ long long table_find(const TableDev& t, uint64_t a, u
   return -1;
 }
 
-// Find or insert.  `inserted` is set when this call created the slot (x = z = 0
-// from the table's initialisation).  Returns -1 only when the probe limit is
-// hit, after raising kErrProbe.
-__device__ __forceinline__ long long table_upsert(const TableDev& t, uint64_t a, uint64_t b, bool& inserted) {
+__device__ __forceinline__ long long table_find(const TableDev& t, uint64_t a, uint64_t b) {
+  const uint64_t i = det_hash(a, b) & t.mask;
+  uint64_t ka, kb;
+  load_key(t.slots + i, ka, kb);
+  return table_find_from(t, a, b, i, ka, kb);
+}
+
+// Find or insert, continuing from a loaded home slot as table_find_from.
+// `inserted` is set when this call created the slot (x = z = 0 from the
+// table's initialisation).  Returns -1 only when the probe limit is hit,
+// after raising kErrProbe.
+__device__ __forceinline__ long long table_upsert_from(const TableDev& t, uint64_t a, uint64_t b, uint64_t i,
+                                                       uint64_t ka, uint64_t kb, bool& inserted) {
   inserted = false;
-  uint64_t i = det_hash(a, b) & t.mask;
   for (int p = 0; p < t.max_probe; ++p) {
-    uint64_t ka, kb;
-    load_key(t.slots + i, ka, kb);
+    if (p > 0) load_key(t.slots + i, ka, kb);
     if (ka == a && kb == b) return static_cast<long long>(i);
     if (ka == kEmptyKey && kb == kEmptyKey) {
       uint64_t oa, ob;
@@ -174,6 +182,13 @@ __device__ __forceinline__ long long table_upsert(const TableDev& t, uint64_t a,
   }
   atomicOr(t.err, kErrProbe);
   return -1;
+}
+
+__device__ __forceinline__ long long table_upsert(const TableDev& t, uint64_t a, uint64_t b, bool& inserted) {
+  const uint64_t i = det_hash(a, b) & t.mask;
+  uint64_t ka, kb;
+  load_key(t.slots + i, ka, kb);
+  return table_upsert_from(t, a, b, i, ka, kb, inserted);
 }
 
 // ---------------------------------------------------------------------------

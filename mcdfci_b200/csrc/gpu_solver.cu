@@ -109,7 +109,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     throw McdError(MCD_ERR_UNSUPPORTED, "num_of_coordinate must be in 1.." + std::to_string(kMaxK) + ".");
   if (opt_.m < 1 || opt_.m > kMaxM)
     throw McdError(MCD_ERR_UNSUPPORTED, "estimate must be in 1.." + std::to_string(kMaxM) + ".");
-  if (opt_.cluster < 0 || opt_.cluster > 16) throw McdError(MCD_ERR_INVALID, "cluster must be in 0..16.");
+  if (opt_.groups < 0) throw McdError(MCD_ERR_INVALID, "groups must be >= 0.");
   zt_ = opt_.z_threshold;
   if (opt_.z_threshold_search && zt_ < 1e-10) zt_ = 1e-10;
 
@@ -153,18 +153,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     own_stream_ = true;
   }
-  // CTAs per column: the largest power of two up to 16 that still lets the
-  // clusters of all k columns be resident at once and leaves every CTA at
-  // least 256 column entries.
-  if (opt_.cluster > 0) {
-    cluster_ = opt_.cluster;
-  } else {
-    cluster_ = 1;
-    for (int c = 2; c <= 16; c *= 2) {
-      if (entries_ < c * 256 || column_max_active_clusters(c, opt_.m) < opt_.k) break;
-      cluster_ = c;
-    }
-  }
+  groups_ = opt_.groups > 0 ? opt_.groups : column_groups(entries_, opt_.k);
+  list_ = column_list_size(opt_.m);
 
   try {
     // Hamiltonian tables in one allocation.
@@ -218,6 +208,12 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     d_occ_ = device_alloc<unsigned long long>(1, "occupancy");
     d_sect_ = device_alloc<unsigned long long>(kLeaderSections, "leader timers");
     check(cudaMemsetAsync(d_sect_, 0, kLeaderSections * sizeof(unsigned long long), stream_), "memset");
+    const size_t parts = static_cast<size_t>(opt_.k) * groups_;
+    d_part_key_ = device_alloc<unsigned long long>(parts * list_, "column partial lists");
+    d_part_slot_ = device_alloc<unsigned>(parts * list_, "column partial lists");
+    d_part_sum_ = device_alloc<double>(parts * 2, "column partial sums");
+    d_done_ = device_alloc<unsigned>(kMaxK, "column tickets");
+    check(cudaMemsetAsync(d_done_, 0, kMaxK * sizeof(unsigned), stream_), "memset");
   } catch (...) {
     release();
     throw;
@@ -234,8 +230,12 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   cl_.st = d_state_;
   cl_.cand_score = d_cand_score_;
   cl_.cand_slot = d_cand_slot_;
+  cl_.part_key = d_part_key_;
+  cl_.part_slot = d_part_slot_;
+  cl_.part_sum = d_part_sum_;
+  cl_.done = d_done_;
   cl_.m = opt_.m;
-  cl_.cluster = cluster_;
+  cl_.groups = groups_;
   cl_.k_grid = opt_.k;
   cl_.na = na_;
   cl_.nb = nb_;
@@ -267,7 +267,15 @@ void GpuSolver::release() {
   cudaFree(d_err_);
   cudaFree(d_occ_);
   cudaFree(d_sect_);
+  cudaFree(d_part_key_);
+  cudaFree(d_part_slot_);
+  cudaFree(d_part_sum_);
+  cudaFree(d_done_);
   d_sect_ = nullptr;
+  d_part_key_ = nullptr;
+  d_part_slot_ = nullptr;
+  d_part_sum_ = nullptr;
+  d_done_ = nullptr;
   d_tables_ = nullptr;
   d_slots_ = nullptr;
   d_state_ = nullptr;

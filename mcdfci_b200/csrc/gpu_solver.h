@@ -27,7 +27,7 @@ struct SolverOptions {
   std::vector<int> ref_det_occ;
   int coordinate_pick = MCD_PICK_GCD_GRAD;
   int coordinate_update = MCD_UPDATE_EIG;
-  int cluster = 0;
+  int groups = 0;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -76,8 +76,8 @@ class GpuSolver {
   Det reference_det() const { return ref_; }
   long long table_capacity() const { return static_cast<long long>(capacity_); }
   unsigned long long max_wavefunction_size() const { return max_size_; }
-  int cluster() const { return cluster_; }
-  int max_active_clusters() const { return column_max_active_clusters(cluster_, opt_.m); }
+  int groups() const { return groups_; }
+  int list_size() const { return list_; }
   int entries_per_column() const { return entries_; }
 
  private:
@@ -91,7 +91,7 @@ class GpuSolver {
   HamHost ham_;
   Det ref_{0, 0};
   double ref_diag_ = 0.0;
-  int na_ = 0, nb_ = 0, entries_ = 0, cluster_ = 1, n_words_ = 1;
+  int na_ = 0, nb_ = 0, entries_ = 0, groups_ = 1, list_ = 32, n_words_ = 1;
   size_t capacity_ = 0;             // hash slots (power of two)
   unsigned long long max_size_ = 0; // reference max_wavefunction_size
   double zt_ = 0.0;
@@ -109,6 +109,10 @@ class GpuSolver {
   unsigned* d_err_ = nullptr;
   unsigned long long* d_occ_ = nullptr;
   unsigned long long* d_sect_ = nullptr;
+  unsigned long long* d_part_key_ = nullptr;
+  unsigned* d_part_slot_ = nullptr;
+  double* d_part_sum_ = nullptr;
+  unsigned* d_done_ = nullptr;
   HamDev hd_{};
   TableDev td_{};
   ColumnLaunch cl_{};

@@ -70,8 +70,12 @@ struct ColumnLaunch {
   IterState* st;
   double* cand_score;     // [kMaxK][m] score of each column's candidates
   unsigned* cand_slot;    // [kMaxK][m] their hash slots (tables have at most 2^32 slots)
+  unsigned long long* part_key;  // [kMaxK][groups][list] per-CTA candidate lists
+  unsigned* part_slot;           // [kMaxK][groups][list]
+  double* part_sum;              // [kMaxK][groups][2] per-CTA new_z and dot partial sums
+  unsigned* done;                // [kMaxK] CTAs finished per column (reset by the last one)
   int m;
-  int cluster;            // CTAs per column
+  int groups;             // CTAs per column
   int k_grid;             // columns launched (>= k_cur)
   int na, nb;             // electrons per spin (fixed by the starting determinant)
 };
@@ -89,16 +93,19 @@ struct LeaderLaunch {
 };
 
 // Phases of the leader kernel timed into LeaderLaunch::sect: 0 state load,
-// 1 finish + prefix, 2 candidate slots, 3 dedupe, 4 refetch, 5 sort, 6 H_sub,
+// 1 finish + prefix, 2 candidate gather (slots, dedupe, scores), 3 top-k,
+// 4 full sort when the k-th score is tied, 5 picked determinants, 6 H_sub,
 // 7 update_x, 8 publish, 9 eig setup, 10 tridiagonalisation, 11 multisection,
 // 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
 // 15 eig finish.
 constexpr int kLeaderSections = 16;
 
 // Launchers (column_kernel.cu / leader_kernel.cu).
-// Clusters of `cluster` column CTAs that fit on the GPU at once.
-int column_max_active_clusters(int cluster, int m);
 int column_entries(int norb, int na, int nb);
+// Length of the per-CTA candidate lists for `estimate` m (32, 64 or 128).
+int column_list_size(int m);
+// CTAs per column for a column of `entries` entries.
+int column_groups(int entries, int k);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
 cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStream_t s);

@@ -25,6 +25,7 @@
 #include "eig.cuh"
 #include "device_common.cuh"
 #include "kernels.h"
+#include "toplist.cuh"
 
 namespace mcd {
 namespace {
@@ -294,10 +295,9 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     if (lane == 0) s_red[warp] = acc;
   }
   __syncthreads();
-  if (tid == 0) {
-    dd t{0, 0};
-    for (int w = 0; w < 32; ++w) t = dd_add(t, s_red[w]);
-    s_rq = t;
+  if (warp == 0) {
+    const dd t = warp_sum_dd(lane < static_cast<int>(blockDim.x >> 5) ? s_red[lane] : dd{0.0, 0.0});
+    if (lane == 0) s_rq = t;
   }
   __syncthreads();
   const dd rq = s_rq;
@@ -360,11 +360,14 @@ __device__ void finish_iteration(IterState* S, const TableDev& T) {
     __threadfence();
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    dd xz = S->xz;
-    for (int c = 0; c < k; ++c) xz = dd_add_d(xz, S->dot[c]);
-    S->xz = xz;
-    S->pending = 0;
+  if (threadIdx.x < 32) {
+    dd acc{0.0, 0.0};
+    for (int c = threadIdx.x; c < k; c += 32) acc = dd_add_d(acc, S->dot[c]);
+    acc = warp_sum_dd(acc);
+    if (threadIdx.x == 0) {
+      S->xz = dd_add(S->xz, acc);
+      S->pending = 0;
+    }
   }
   __syncthreads();
 }
@@ -405,6 +408,43 @@ __device__ __forceinline__ int block_rank(bool keep, int* wsum, int* chunk_total
 }
 
 constexpr unsigned kNoSlot = 0xFFFFFFFFu;
+
+// The k best (score, slot) pairs among n candidates (us, sc in shared
+// memory), k < 32R.  Each warp keeps a top-32R list of its share; the lists
+// merge as a tree in `scratch` (which may alias us and sc: it is written only
+// after every warp has read them).  Writes the k slots in order of decreasing
+// score and returns false when the k-th and (k+1)-th scores are equal, so that
+// the caller can order that tie by determinant.
+template <int R>
+__device__ bool topk_fast(const unsigned* us, const double* sc, int n, int k, unsigned char* scratch,
+                          unsigned* out) {
+  __shared__ int s_tie;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  TopList<R> T;
+  toplist_clear<R>(T);
+  for (int base = warp * 32; base < n; base += blockDim.x) {
+    const int u = base + lane;
+    const unsigned long long key =
+        u < n ? static_cast<unsigned long long>(__double_as_longlong(sc[u])) + 1ull : 0ull;
+    toplist_offer<R>(T, key, u < n ? us[u] : 0u);
+  }
+  __syncthreads();
+  unsigned long long* skey = reinterpret_cast<unsigned long long*>(scratch);
+  unsigned* spay = reinterpret_cast<unsigned*>(skey + (blockDim.x >> 5) * 32 * R);
+  toplist_cta_merge<R>(T, skey, spay);
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < R; ++j)
+      if (j * 32 + lane < k) out[j * 32 + lane] = T.p[j];
+    if (lane == 0) {
+      const unsigned long long a = skey[k - 1], b = skey[k];
+      s_tie = (b != 0ull && a == b) ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  return s_tie == 0;
+}
+
 
 __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -475,26 +515,28 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
     return;
   }
 
-  // 2. Candidate slots; duplicates (one determinant in several columns) removed
-  //    with a shared-memory hash set.
+  // 2-3. Candidate slots, with duplicates (one determinant in several
+  //      columns) removed through a shared-memory hash set, and their scores
+  //      |x*xx*scale^2 + z| refetched from the table.
   const int R = s_R;
   int PR = 2;  // >= 2 keeps the score array (which reuses the hash set) 8-byte aligned
   while (PR < R) PR <<= 1;
-  unsigned* us = reinterpret_cast<unsigned*>(smem);          // [PR] slots, compacted in place
-  unsigned* hs = us + PR;                                     // [2*PR] hash set; later scores (double[PR])
+  unsigned* us = reinterpret_cast<unsigned*>(smem);  // [PR] slots, compacted in place
+  unsigned* hs = us + PR;                             // [2*PR] hash set; then scores (double[PR])
+  double* sc = reinterpret_cast<double*>(hs);
   const int H = 2 * PR;
-  for (int i = tid; i < H; i += kLT) hs[i] = kNoSlot;
-  for (int r = tid; r < R; r += kLT) {
-    int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (s_off[mid] <= r) lo = mid; else hi = mid;
+  const dd xss = sS.xss;
+  auto gather = [&]() {
+    for (int i = tid; i < H; i += kLT) hs[i] = kNoSlot;
+    for (int r = tid; r < R; r += kLT) {
+      int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_off[mid] <= r) lo = mid; else hi = mid;
+      }
+      us[r] = L.cand_slot[lo * m + (r - s_off[lo])];
     }
-    us[r] = L.cand_slot[lo * m + (r - s_off[lo])];
-  }
-  __syncthreads();
-  clk.mark(2);
-  {
+    __syncthreads();
     int total = 0;
     for (int base = 0; base < R; base += kLT) {
       const int r = base + tid;
@@ -519,79 +561,94 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
       __syncthreads();
     }
     if (tid == 0) s_U = total;
-  }
-  __syncthreads();
-  clk.mark(3);
-  const int U = s_U;
-  int P = 1;
-  while (P < U) P <<= 1;
-
-  // 3. Scores of the unique candidates from the table (refetch).
-  double* sc = reinterpret_cast<double*>(hs);  // [P]
-  const dd xss = sS.xss;
-  for (int u = tid; u < P; u += kLT) {
-    if (u < U) {
-      const Slot* sp = T.slots + us[u];
-      const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
-      const double g = score_of(x, z, xss);
-      sc[u] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the padding
-    } else {
-      sc[u] = -1.0;
-      us[u] = kNoSlot;
+    __syncthreads();
+    const int Ul = s_U;
+    int Pl = 1;
+    while (Pl < Ul) Pl <<= 1;
+    for (int u = tid; u < Pl; u += kLT) {
+      if (u < Ul) {
+        const Slot* sp = T.slots + us[u];
+        const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
+        const double g = score_of(x, z, xss);
+        sc[u] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the padding
+      } else {
+        sc[u] = -1.0;
+        us[u] = kNoSlot;
+      }
     }
-  }
-  __syncthreads();
-  clk.mark(4);
+    __syncthreads();
+  };
+  gather();
+  clk.mark(2);
+  const int U = s_U;
+  const int k = U < L.k_req ? U : L.k_req;
 
-  // 4. Bitonic sort, highest priority first: larger score, then the larger
-  //    determinant in the reference order (ties between different
-  //    determinants read their keys from the table).
-  const int nwords = sS.n_words;
-  for (int size = 2; size <= P; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = tid; t < (P >> 1); t += kLT) {
-        const int i = 2 * stride * (t / stride) + (t % stride);
-        const int j = i + stride;
-        const double si = sc[i], sj = sc[j];
-        bool jfirst;
-        if (si != sj) {
-          jfirst = sj > si;
-        } else {
-          const unsigned a = us[i], b = us[j];
-          if (a == kNoSlot || b == kNoSlot || a == b) {
-            jfirst = false;
+  // 4. The k largest scores: per-warp top lists over the candidates, merged
+  //    as a tree.  Equal scores are ordered by the reference's determinant
+  //    order (detComp_global, src/wavefunction.h:30-36); when the k-th and
+  //    (k+1)-th scores are equal that order decides the set, and the whole
+  //    candidate list is sorted instead (rare).
+  bool fast;
+  if (k < 32)
+    fast = topk_fast<1>(us, sc, U, k, smem, s_slot);
+  else if (k < 64)
+    fast = topk_fast<2>(us, sc, U, k, smem, s_slot);
+  else if (k < 128)
+    fast = topk_fast<4>(us, sc, U, k, smem, s_slot);
+  else
+    fast = topk_fast<8>(us, sc, U, k, smem, s_slot);
+  clk.mark(3);
+  if (!fast) {
+    gather();
+    int P = 1;
+    while (P < U) P <<= 1;
+    const int nwords = sS.n_words;
+    for (int size = 2; size <= P; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = tid; t < (P >> 1); t += kLT) {
+          const int i = 2 * stride * (t / stride) + (t % stride);
+          const int j = i + stride;
+          const double si = sc[i], sj = sc[j];
+          bool jfirst;
+          if (si != sj) {
+            jfirst = sj > si;
           } else {
-            uint64_t ia, ib, ja, jb;
-            load_key(T.slots + a, ia, ib);
-            load_key(T.slots + b, ja, jb);
-            jfirst = det_ref_compare(ja, jb, ia, ib, nwords) > 0;
+            const unsigned a = us[i], b = us[j];
+            if (a == kNoSlot || b == kNoSlot || a == b) {
+              jfirst = false;
+            } else {
+              uint64_t ia, ib, ja, jb;
+              load_key(T.slots + a, ia, ib);
+              load_key(T.slots + b, ja, jb);
+              jfirst = det_ref_compare(ja, jb, ia, ib, nwords) > 0;
+            }
+          }
+          const bool up = (i & size) == 0;
+          if (jfirst == up) {
+            sc[i] = sj;
+            sc[j] = si;
+            const unsigned tmp = us[i];
+            us[i] = us[j];
+            us[j] = tmp;
           }
         }
-        const bool up = (i & size) == 0;
-        if (jfirst == up) {
-          sc[i] = sj;
-          sc[j] = si;
-          const unsigned tmp = us[i];
-          us[i] = us[j];
-          us[j] = tmp;
-        }
+        __syncthreads();
       }
-      __syncthreads();
     }
+    if (tid < k) s_slot[tid] = us[tid];
+    __syncthreads();
   }
-  clk.mark(5);
-  const int k = U < L.k_req ? U : L.k_req;
+  clk.mark(4);
   if (tid < k) {
-    const unsigned slot = us[tid];
-    const Slot* sp = T.slots + slot;
+    const Slot* sp = T.slots + s_slot[tid];
     uint64_t a, b;
     load_key(sp, a, b);
-    s_slot[tid] = slot;
     s_det[tid] = Det{a, b};
     s_x[tid] = load_relaxed(&sp->x);
     s_z[tid] = load_relaxed(&sp->z);
   }
   __syncthreads();
+  clk.mark(5);
 
   // 5. H_sub: in shared memory when it fits beside the eig scratch, else in
   //    the global copy (which is written either way for inspection).
@@ -640,14 +697,18 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
   clk.mark(7);
 
   // 8. Publish the next iteration.
-  if (tid == 0) {
-    dd xz = sS.xz;
-    double mx = 0.0;
-    for (int i = 0; i < k; ++i) {
-      xz = dd_add_d(xz, s_z[i] * s_dx[i]);
+  dd zdx{0.0, 0.0};
+  double mx = 0.0;
+  if (warp == 0) {
+    for (int i = lane; i < k; i += 32) {
+      zdx = dd_add_d(zdx, s_z[i] * s_dx[i]);
       mx = fmax(mx, fabs(s_dx[i]));
     }
-    G->xz = xz;
+    zdx = warp_sum_dd(zdx);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(~0u, mx, o));
+  }
+  if (tid == 0) {
+    G->xz = dd_add(sS.xz, zdx);
     G->xx = er.xx;
     G->scale = er.scale;
     G->xss = dd_mul(er.xx, dd_mul(er.scale, er.scale));
@@ -743,7 +804,9 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, const double* 
 size_t leader_smem_bytes(int k, int m) {
   size_t P = 2;
   while (P < static_cast<size_t>(k) * m) P <<= 1;
-  const size_t pick = P * 4 + 2 * P * 4;  // slots + hash set (the hash set area later holds P doubles)
+  size_t pick = P * 4 + 2 * P * 4;  // slots + hash set (the hash set area later holds P doubles)
+  const size_t lists = static_cast<size_t>(kLT / 32) * 32 * (k < 32 ? 1 : k < 64 ? 2 : k < 128 ? 4 : 8) * 12;
+  if (lists > pick) pick = lists;  // top-k merge scratch, aliasing the candidate arrays
   const size_t hs = (k <= 64 ? static_cast<size_t>(k) * k : 0) * sizeof(double);
   const size_t eig = hs + eig_work_doubles(k) * sizeof(double);
   return pick > eig ? pick : eig;

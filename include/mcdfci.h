@@ -176,6 +176,23 @@ int mcd_debug_hsub(mcd_solver* s, const uint64_t* alpha, const uint64_t* beta, i
  * and the branch (1: (k+1)x(k+1) problem, 2: k x k first-iteration problem). */
 int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                   const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch);
+/* mcd_debug_eig without any allocation: no counterpart in the reference.
+ * The same kernel and results, but its device buffers are a file-scope
+ * static device array of 134 KB (k <= 128; a larger k returns
+ * MCD_ERR_UNSUPPORTED) instead of cudaMalloc/cudaFree per call, for callers
+ * that cannot allocate: a host whose device memory is committed to the hash
+ * wavefunction, or one that cannot take the device-wide synchronisation of
+ * cudaFree while a solver runs on another stream.  Inputs and outputs are
+ * host buffers; the call runs on `stream` (NULL = the legacy default stream)
+ * on the current device and synchronises that stream before it returns.
+ * The first call on each device finds the array's address and sets the
+ * kernel's shared-memory limit: make it before any stream capture on that
+ * device.  The kernel writes every output word on each call, so nothing has
+ * to start at zero.  Calls that overlap on one device (two host threads)
+ * share the array and race: serialise them. */
+int mcd_eig_update_static(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                          const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch,
+                          void* stream);
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);

@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
     "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_launch_info", "mcd_debug_leader_sections",
+    "mcd_eig_update_static",
 )
 
 
@@ -128,6 +129,8 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_hsub.argtypes = [vp, _u64p, _u64p, ctypes.c_int32, _dp]
     L.mcd_debug_eig.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                 ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_eig_update_static.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                        ctypes.POINTER(ctypes.c_int32), vp]
     L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
@@ -435,6 +438,26 @@ def debug_eig(hsub, x, z, xx, xz):
     _check(library().mcd_debug_eig(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
                                    xxa, xza, dx.ctypes.data_as(_dp), nxx, nsc, ctypes.byref(br)))
     return dx, tuple(nxx), tuple(nsc), br.value
+
+
+def eig_update_static(hsub, x, z, xx, xz, stream=None):
+    """debug_eig without allocation (mcd_eig_update_static): the device
+    buffers are a static array in the library, k <= 128.  Same returns."""
+    import numpy as np
+
+    hsub = np.ascontiguousarray(hsub, dtype=np.float64)
+    k = hsub.shape[0]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    dx = np.zeros(max(k, 1))
+    nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+    br = ctypes.c_int32()
+    xxa = (ctypes.c_double * 2)(*xx)
+    xza = (ctypes.c_double * 2)(*xz)
+    _check(library().mcd_eig_update_static(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
+                                           z.ctypes.data_as(_dp), xxa, xza, dx.ctypes.data_as(_dp), nxx, nsc,
+                                           ctypes.byref(br), stream))
+    return dx[:k], tuple(nxx), tuple(nsc), br.value
 
 
 def run_json(path: str) -> int:

@@ -425,6 +425,31 @@ int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* 
   });
 }
 
+int mcd_eig_update_static(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                          const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch,
+                          void* stream) {
+  return guarded([&] {
+    if (k < 1 || k > mcd::kStaticEigMaxK)
+      return fail(MCD_ERR_UNSUPPORTED, "mcd_eig_update_static: k = " + std::to_string(k) +
+                                           " is outside 1..128, the size of its static device scratch.");
+    if (!hsub || !x || !z || !xx || !xz || !dx || !new_xx || !new_scale)
+      return fail(MCD_ERR_INVALID, "mcd_eig_update_static: NULL argument.");
+    mcd::dd out[2];
+    int br = 0;
+    unsigned err = 0;
+    const cudaError_t e = mcd::eig_update_static(k, hsub, x, z, mcd::dd{xx[0], xx[1]}, mcd::dd{xz[0], xz[1]}, dx,
+                                                 out, &br, &err, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(MCD_ERR_CUDA, cudaGetErrorString(e));
+    new_xx[0] = out[0].hi;
+    new_xx[1] = out[0].lo;
+    new_scale[0] = out[1].hi;
+    new_scale[1] = out[1].lo;
+    if (branch) *branch = br;
+    if (err) return fail(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");

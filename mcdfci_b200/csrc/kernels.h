@@ -129,4 +129,12 @@ cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* 
                       double* dx, dd* xx_scale, int* branch, unsigned* err, cudaStream_t s);
 size_t leader_smem_bytes(int k, int m);
 
+// debug_eig on HOST buffers with its device buffers in a file-scope device
+// array (leader_kernel.cu) instead of cudaMalloc: no allocation.  k <= 128;
+// returns cudaErrorInvalidValue above.  Runs on stream s and synchronises it.
+// Calls that overlap on one device share the array and race.
+constexpr int kStaticEigMaxK = 128;
+cudaError_t eig_update_static(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
+                              double* dx, dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s);
+
 }  // namespace mcd

@@ -22,6 +22,8 @@
 //                          (WaveFunctionCuckoo::update_x, src/wavefunction.h:425-451)
 //   publish                the k picked determinants, dx, H_cc, xx*scale^2
 //                          and scale for the column kernel.
+#include <mutex>
+
 #include "eig.cuh"
 #include "device_common.cuh"
 #include "kernels.h"
@@ -848,6 +850,104 @@ cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* 
   if (e != cudaSuccess) return e;
   debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// eig_update_static: the eig update of debug_eig run on a file-scope device
+// array instead of cudaMalloc'd buffers.  Layout in doubles: H [kStaticEigMaxK^2],
+// x, z, dx [kStaticEigMaxK each], new xx and scale as two dd, then one word
+// holding the branch (int) and the error word (unsigned).  static_eig_kernel
+// writes dx[0..k), both dd, the branch and the error word on every launch, so
+// no part of the array has to start at zero or be cleared between calls.
+
+namespace {
+
+constexpr size_t kStaticEigH = 0;
+constexpr size_t kStaticEigX = kStaticEigH + static_cast<size_t>(kStaticEigMaxK) * kStaticEigMaxK;
+constexpr size_t kStaticEigZ = kStaticEigX + kStaticEigMaxK;
+constexpr size_t kStaticEigDx = kStaticEigZ + kStaticEigMaxK;
+constexpr size_t kStaticEigOut = kStaticEigDx + kStaticEigMaxK;  // 2 dd = 4 doubles
+constexpr size_t kStaticEigFlags = kStaticEigOut + 4;            // int branch, unsigned err
+constexpr size_t kStaticEigDoubles = kStaticEigFlags + 1;
+
+static __device__ __align__(256) double g_static_eig_scratch[kStaticEigDoubles];
+
+// debug_eig_kernel on the array at `base` (the address of
+// g_static_eig_scratch on this device).  A kernel of its own, so that its
+// shared-memory attribute, set once per device, is not changed by debug_eig.
+__global__ void __launch_bounds__(kLT, 1) static_eig_kernel(int k, double* base, dd xx, dd xz) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    s_x[i] = base[kStaticEigX + i];
+    s_z[i] = base[kStaticEigZ + i];
+  }
+  __syncthreads();
+  SectionClock clk{nullptr, 0};
+  const EigResult er = eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
+  for (int i = threadIdx.x; i < k; i += blockDim.x) base[kStaticEigDx + i] = s_dx[i];
+  if (threadIdx.x == 0) {
+    dd* out = reinterpret_cast<dd*>(base + kStaticEigOut);
+    out[0] = er.xx;
+    out[1] = er.scale;
+    int* flags = reinterpret_cast<int*>(base + kStaticEigFlags);
+    flags[0] = er.branch;
+    flags[1] = er.ok ? 0 : static_cast<int>(kErrEig);
+  }
+}
+
+constexpr int kStaticEigMaxDevices = 64;
+std::mutex g_static_eig_mutex;
+double* g_static_eig_base[kStaticEigMaxDevices] = {};
+
+// Once per device, with that device current: the address of the array in
+// this device's copy of the module, and the shared-memory attribute of the
+// kernel for the largest k.
+cudaError_t static_eig_setup(double** base) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kStaticEigMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_static_eig_mutex);
+  if (!g_static_eig_base[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_eig_scratch);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(static_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(eig_work_doubles(kStaticEigMaxK) * sizeof(double)));
+    if (e != cudaSuccess) return e;
+    g_static_eig_base[dev] = static_cast<double*>(p);
+  }
+  *base = g_static_eig_base[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t eig_update_static(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
+                              double* dx, dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
+  if (k < 1 || k > kStaticEigMaxK) return cudaErrorInvalidValue;  // the caller reports the limit
+  double* base = nullptr;
+  cudaError_t e = static_eig_setup(&base);
+  if (e != cudaSuccess) return e;
+  double* dH = base + kStaticEigH;
+  double* dX = base + kStaticEigX;
+  double* dZ = base + kStaticEigZ;
+  double* dDx = base + kStaticEigDx;
+  dd* dOut = reinterpret_cast<dd*>(base + kStaticEigOut);
+  int* dBranch = reinterpret_cast<int*>(base + kStaticEigFlags);
+  unsigned* dErr = reinterpret_cast<unsigned*>(dBranch + 1);
+  const size_t kk = static_cast<size_t>(k);
+  if ((e = cudaMemcpyAsync(dH, hsub, sizeof(double) * kk * kk, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(dX, x, sizeof(double) * kk, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(dZ, z, sizeof(double) * kk, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  static_eig_kernel<<<1, kLT, eig_work_doubles(k) * sizeof(double), s>>>(k, base, xx, xz);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(dx, dDx, sizeof(double) * kk, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(new_xx_scale, dOut, sizeof(dd) * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(branch, dBranch, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(err, dErr, sizeof(unsigned), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
 }
 
 }  // namespace mcd

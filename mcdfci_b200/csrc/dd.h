@@ -83,12 +83,16 @@ DD_HD dd dd_mul_d(dd a, double b) {
   return dd_fast_two_sum(p.hi, p.lo);
 }
 
+// Three quotient digits q1 + q2 + q3 from one reciprocal of b.hi: each digit
+// is a double estimate of the remaining quotient and the exact remainder
+// carries its error to the next one.
 DD_HD dd dd_div(dd a, dd b) {
-  double q1 = a.hi / b.hi;
+  const double rb = 1.0 / b.hi;
+  double q1 = a.hi * rb;
   dd r = dd_sub(a, dd_mul_d(b, q1));
-  double q2 = r.hi / b.hi;
+  double q2 = r.hi * rb;
   r = dd_sub(r, dd_mul_d(b, q2));
-  double q3 = r.hi / b.hi;
+  double q3 = r.hi * rb;
   dd q = dd_fast_two_sum(q1, q2);
   return dd_add_d(q, q3);
 }

@@ -1,26 +1,33 @@
-// Smallest eigenpair of a small dense symmetric FP64 matrix, computed by one
-// CTA of 1024 threads in shared memory.
+// Lowest eigenpair of a small dense symmetric FP64 matrix (n <= kMaxK+1),
+// computed in shared memory by one CTA of kEigThreads threads.
 //
 // The reference calls LAPACK dsyevr (IL=IU=1) and refines the vector with one
 // step of __float128 inverse iteration through dgetrf (src/solver.h:400-503).
-// Here, for n <= kMaxK+1:
+// Here the work is arranged around the serial dependencies of one CTA:
 //   1. Householder reduction to tridiagonal T = Q^T A Q (Golub & Van Loan,
-//      Algorithm 8.3.1).  Each step takes two CTA barriers: every warp derives
-//      the reflector scalars from the current column itself (identical
-//      arithmetic in every warp, so no broadcast barrier), forms p = beta A v
-//      for its rows, then, after a barrier, K = beta/2 p'v and the rank-2
-//      update of its rows.  Reflector j is kept in row j right of the diagonal,
-//      which the reduction never reads again.
-//   2. The lowest eigenvalue of T is isolated by 1024-way multisection: each
-//      thread counts the eigenvalues below its shift from the signs of the
-//      characteristic polynomials of the leading sub-matrices (Sturm's
-//      theorem), computed by the three-term recurrence with power-of-two
-//      rescaling, four rounds.
+//      Algorithm 8.3.1) by the first ceil((n-1)/32) warps, one pass over the
+//      trailing rows per step: the next pivot row is updated first, one
+//      column per thread, every thread derives the next reflector from two
+//      sums, and then each thread updates its own row with reflector j while
+//      forming its element of p = tau A u for reflector j+1.  Reflector j is
+//      H_j = I - tau_j u_j u_j^T with u_j = (0..0, A[j][j+1..n)), where
+//      A[j][j+1] holds u0_j; row j is not written after step j.
+//   2. The lowest eigenvalue of T is bracketed by 128-way multisection on four
+//      warps (one per SM sub-partition): T - sigma I is positive definite
+//      exactly when every leading principal minor is positive (Sylvester), and
+//      the minors follow p_{i+1} = (d_i - sigma) p_i - e_{i-1}^2 p_{i-1}.
+//      Meanwhile the other warps form M[i][j] = tau_i u_j^T u_i (j < i) in
+//      the lower triangle of A, which the reduction no longer reads.
 //   3. Inverse iteration on T - sigma I with sigma at the lower end of the
-//      isolating interval (positive definite, so no pivoting), three solves.
-//   4. Back-transformation v = Q y by warp 0 with y in registers.
-// The caller forms the Rayleigh quotient in double-double from the original
-// matrix, which is the quantity the reference's refined step approximates
+//      bracket (positive definite, so LU without pivoting is stable).  The LU
+//      pivots are the ratios p_{i+1}/p_i of the same minors: one FMA
+//      recurrence, then independent divisions.
+//   4. Back-transformation v = H_0 H_1 ... H_{n-3} y without a chain of
+//      reductions: with c_j = u_j^T y, the coefficients s_j of
+//      v = y - sum_j tau_j s_j u_j solve s_j = c_j - sum_{i>j} M[i][j] s_i,
+//      a triangular solve of one shuffle and one FMA per step.
+// The caller forms the Rayleigh quotient from the original matrix, the
+// quantity that the reference's refined step approximates
 // (rq = v'Bv + 2 dv'Bv, src/solver.h:516-521).
 #pragma once
 
@@ -29,122 +36,237 @@
 namespace mcd {
 
 constexpr int kEigThreads = 1024;
+constexpr int kEigBracketWarps = 4;
+constexpr int kEigBracketRounds = 5;  // 129^5 = 3.6e10 : 1 reduction of the Gershgorin interval
 
-struct EigScratch {
-  double* A;     // n x n, row-major, leading dimension lda
-  int lda;
-  double* d;     // [n] diagonal of T
-  double* e;     // [n] sub-diagonal of T
-  double* e2;    // [n] e^2
-  double* beta;  // [n] reflector coefficients
-  double* hv;    // [n] scratch
-  double* p;     // [n] scratch
-  double* y;     // [n] eigenvector (output)
-  double* part;  // [32] per-warp partials
-  double* scal;  // [8] scalars
-  int* ibest;    // [1]
-};
+// Leading dimension of an n x n work matrix: odd, so that the lanes of a warp
+// reading one column of consecutive rows hit distinct shared-memory banks.
+__host__ __device__ constexpr int eig_lda(int n) { return n | 1; }
 
-// Reflector scalars of column j (rows j+1..n-1), computed identically by
-// every lane of every warp: beta, 1/v0 and the new sub-diagonal mu.
-__device__ __forceinline__ void house_scalars(const double* A, int lda, int j, int m, double& bet, double& inv_v0,
-                                              double& mu) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int i = 1 + lane; i < m; i += 32) {
-    const double v = A[(j + 1 + i) * lda + j];
-    s = fma(v, v, s);
-  }
-  s = __shfl_sync(~0u, warp_sum(s), 0);
-  const double x0 = A[(j + 1) * lda + j];
-  bet = 0.0;
-  inv_v0 = 0.0;
-  mu = x0;
-  if (s != 0.0) {
-    mu = sqrt(x0 * x0 + s);
-    const double v0 = (x0 <= 0.0) ? x0 - mu : -s / (x0 + mu);
-    bet = 2.0 * v0 * v0 / (s + v0 * v0);
-    inv_v0 = 1.0 / v0;
-  }
+__device__ __forceinline__ void bar_named(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Block-wide.  On return ws.y[0..n) holds an (unnormalised) eigenvector of the
-// lowest eigenvalue of the matrix originally in ws.A; ws.A is overwritten.
-__device__ void smallest_eigvec(EigScratch& ws, int n, SectionClock& clk) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int NT = blockDim.x;
-  const int NW = NT >> 5;
-  double* A = ws.A;
-  const int lda = ws.lda;
+// Per-index vectors of the solver, n doubles each.
+struct EigVecs {
+  double *d, *e, *e2;  // diagonal, sub-diagonal and its squares of T
+  double *u0, *tau;    // reflectors
+  double *num, *den;   // p and w vectors of the reduction; then the minors p_{i+1}, p_i at sigma
+  double *ru, *l;      // LU of T - sigma I: 1 / pivot, multipliers
+  double *y;           // eigenvector of T, then of A
+  double *c, *g;       // back-transformation: u_j^T y and tau_j s_j
+};
 
-  if (n == 1) {
-    if (tid == 0) ws.y[0] = 1.0;
-    __syncthreads();
+// Householder scalars for x = (x0, rest) with |rest|^2 = s: u = x + sign(x0)
+// mu e_1 maps x to e e_1 with e = -sign(x0) mu; u'u = 2 mu |u0|, tau = 2/u'u.
+__device__ __forceinline__ void eig_reflector(double x0, double s, double& u0, double& tau, double& e) {
+  if (s == 0.0) {  // nothing to annihilate: H = I
+    u0 = 0.0;
+    tau = 0.0;
+    e = x0;
+    return;
+  }
+  const double mu = sqrt(fma(x0, x0, s));
+  const double sg = x0 < 0.0 ? -1.0 : 1.0;
+  u0 = fma(sg, mu, x0);
+  tau = 1.0 / (mu * fabs(u0));
+  e = -sg * mu;
+}
+
+// 1. Tridiagonalisation; threads [0, 32*nwa) only, 32*nwa >= n-1, n >= 2.
+// Step j, with reflector j, p = tau_j A u_j and K = tau_j/2 p'u_j known:
+//   (a) w = p - K u_j, one column per thread;
+//   (b) row j+1 after the update, one column per thread: its diagonal is
+//       d_{j+1}, the rest defines reflector j+1, whose scalars every thread
+//       derives from two sums;
+//   (c) rows j+2.. after the update, one row per thread, in the same pass as
+//       p = tau_{j+1} A u_{j+1}.
+// A[j][j+1] is replaced by u0_j, so u_j is row j from column j+1 on.
+__device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const EigVecs& V, int nwa) {
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int T = 32 * nwa;
+  double* const P = V.num;
+  double* const W = V.den;
+  __shared__ double s_red[2][kEigBracketWarps][2];
+  // Sums of a and b over the participating threads, identical in all of them.
+  auto sum2 = [&](double& a, double& b, int buf) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (nwa > 1) {
+      if (lane == 0) {
+        s_red[buf][wid][0] = a;
+        s_red[buf][wid][1] = b;
+      }
+      bar_named(1, T);
+      a = 0.0;
+      b = 0.0;
+      for (int q = 0; q < nwa; ++q) {
+        a += s_red[buf][q][0];
+        b += s_red[buf][q][1];
+      }
+    }
+  };
+  auto sync = [&]() {
+    if (nwa == 1)
+      __syncwarp();
+    else
+      bar_named(1, T);
+  };
+  if (n == 2) {
+    if (t == 0) {
+      V.d[0] = A[0];
+      V.e[0] = A[1];
+      V.d[1] = A[lda + 1];
+    }
     return;
   }
 
-  // 1. Tridiagonalisation.
-  for (int j = 0; j + 2 < n; ++j) {
-    const int m = n - j - 1;
-    double bet, inv_v0, mu;
-    house_scalars(A, lda, j, m, bet, inv_v0, mu);
-    if (tid == 0) {
-      ws.beta[j] = bet;
-      ws.e[j] = mu;
-      ws.d[j] = A[j * lda + j];
+  // Reflector 0 from row 0; p and K of step 0.
+  double tau, K;
+  {
+    const int c = 1 + t;
+    const double a = c < n ? A[c] : 0.0;
+    double sq = (c >= 2 && c < n) ? a * a : 0.0;
+    double x0 = (c == 1) ? a : 0.0;
+    sum2(sq, x0, 0);
+    double u0, e0;
+    eig_reflector(x0, sq, u0, tau, e0);
+    if (t == 0) {
+      V.d[0] = A[0];
+      V.e[0] = e0;
+      V.u0[0] = u0;
+      V.tau[0] = tau;
+      A[1] = u0;
     }
-    if (bet == 0.0) continue;  // column already reduced; T keeps e[j] = x0
-    const double* colj = A + (j + 1) * lda + j;  // element i at colj[i * lda]
-    // p = beta * A22 * v for this warp's rows.
-    for (int r = warp; r < m; r += NW) {
-      const double* row = A + (j + 1 + r) * lda + (j + 1);
-      double acc = 0.0;
-      for (int c = lane; c < m; c += 32) {
-        const double hc = (c == 0) ? 1.0 : colj[c * lda] * inv_v0;
-        acc = fma(row[c], hc, acc);
+    sync();
+    const int r = 1 + t;
+    double p = 0.0, ur = 0.0;
+    if (r < n) {
+      const double* Rr = A + r * lda;
+      double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+      int cc = 1;
+      for (; cc + 3 < n; cc += 4) {
+        p0 = fma(Rr[cc], A[cc], p0);
+        p1 = fma(Rr[cc + 1], A[cc + 1], p1);
+        p2 = fma(Rr[cc + 2], A[cc + 2], p2);
+        p3 = fma(Rr[cc + 3], A[cc + 3], p3);
       }
-      acc = warp_sum(acc);
-      if (lane == 0) ws.p[r] = bet * acc;
+      for (; cc < n; ++cc) p0 = fma(Rr[cc], A[cc], p0);
+      p = tau * ((p0 + p1) + (p2 + p3));
+      ur = A[r];
+      P[r] = p;
     }
-    __syncthreads();
-    // K = beta/2 * p'v (identical in every warp), then A22 -= v w' + w v'.
-    double kp = 0.0;
-    for (int r = lane; r < m; r += 32) {
-      const double hr = (r == 0) ? 1.0 : colj[r * lda] * inv_v0;
-      kp = fma(ws.p[r], hr, kp);
-    }
-    const double K = 0.5 * bet * __shfl_sync(~0u, warp_sum(kp), 0);
-    for (int r = warp; r < m; r += NW) {
-      const double hr = (r == 0) ? 1.0 : colj[r * lda] * inv_v0;
-      const double wr = ws.p[r] - K * hr;
-      double* row = A + (j + 1 + r) * lda + (j + 1);
-      for (int c = lane; c < m; c += 32) {
-        const double hc = (c == 0) ? 1.0 : colj[c * lda] * inv_v0;
-        const double wc = ws.p[c] - K * hc;
-        row[c] -= hr * wc + wr * hc;
-      }
-    }
-    if (warp == NW - 1)
-      for (int c = lane; c < m; c += 32) A[j * lda + (j + 1 + c)] = (c == 0) ? 1.0 : colj[c * lda] * inv_v0;
-    __syncthreads();
+    double kp = p * ur, zero = 0.0;
+    sum2(kp, zero, 1);
+    K = 0.5 * tau * kp;
   }
-  if (tid == 0) {
-    ws.d[n - 2] = A[(n - 2) * lda + (n - 2)];
-    ws.e[n - 2] = A[(n - 1) * lda + (n - 2)];
-    ws.d[n - 1] = A[(n - 1) * lda + (n - 1)];
-  }
-  __syncthreads();
-  clk.mark(10);
 
-  // 2. Multisection for the lowest eigenvalue of T.
+  for (int j = 0; j + 2 < n; ++j) {
+    const double* Uj = A + j * lda;  // u_j from column j+1
+    double* R1 = A + (j + 1) * lda;  // the next pivot row
+    const bool more = j + 3 < n;     // reflector j+1 exists
+    // (a)
+    const int c = j + 1 + t;
+    double uc = 0.0, wc = 0.0;
+    if (c < n) {
+      uc = Uj[c];
+      wc = fma(-K, uc, P[c]);
+      W[c] = wc;
+    }
+    sync();
+    // (b)
+    const double u1 = Uj[j + 1], w1 = W[j + 1];
+    double a = 0.0;
+    if (c < n) a = fma(-u1, wc, fma(-w1, uc, R1[c]));
+    double sq = (c >= j + 3 && c < n) ? a * a : 0.0;
+    double x0 = (c == j + 2) ? a : 0.0;
+    sum2(sq, x0, 0);
+    double u0n = 0.0, taun = 0.0, en = x0;
+    if (more) eig_reflector(x0, sq, u0n, taun, en);
+    if (c == j + 1) V.d[j + 1] = a;
+    if (t == 0) {
+      V.e[j + 1] = en;
+      if (more) {
+        V.u0[j + 1] = u0n;
+        V.tau[j + 1] = taun;
+      }
+    }
+    if (c >= j + 2 && c < n) R1[c] = (c == j + 2 && more) ? u0n : a;
+    sync();
+    // (c)
+    const int r = j + 2 + t;
+    double pn = 0.0, urn = 0.0;
+    if (r < n) {
+      double* Rr = A + r * lda;
+      const double ur = Uj[r], wr = W[r];
+      double p0 = 0.0, p1 = 0.0;
+      int cc = j + 2;
+      for (; cc + 3 < n; cc += 4) {
+        double x[4], uj[4], wv[4], un[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          x[q] = Rr[cc + q];
+          uj[q] = Uj[cc + q];
+          wv[q] = W[cc + q];
+          un[q] = R1[cc + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          x[q] = fma(-ur, wv[q], fma(-wr, uj[q], x[q]));
+          Rr[cc + q] = x[q];
+        }
+        p0 = fma(x[0], un[0], p0);
+        p1 = fma(x[1], un[1], p1);
+        p0 = fma(x[2], un[2], p0);
+        p1 = fma(x[3], un[3], p1);
+      }
+      for (; cc < n; ++cc) {
+        const double xv = fma(-ur, W[cc], fma(-wr, Uj[cc], Rr[cc]));
+        Rr[cc] = xv;
+        p0 = fma(xv, R1[cc], p0);
+      }
+      pn = taun * (p0 + p1);
+      urn = R1[r];
+      if (more) P[r] = pn;
+      if (!more) V.d[n - 1] = Rr[n - 1];  // r == n-1: the last diagonal
+    }
+    if (more) {
+      double kp = pn * urn, zero = 0.0;
+      sum2(kp, zero, 1);
+      K = 0.5 * taun * kp;
+    }
+    tau = taun;
+    sync();
+  }
+}
+
+// Rescales a pair of consecutive minors by a power of two when the newer one
+// leaves [1e-150, 1e150]; signs and the ratio are unchanged.  Called every
+// four recurrence steps, which grow the magnitudes by far less than 1e150.
+__device__ __forceinline__ void pair_rescale(double& pc, double& pm) {
+  const double a = fabs(pc);
+  const double f = a > 1e150 ? 0x1p-500 : (a < 1e-150 && a > 0.0 ? 0x1p+500 : 1.0);
+  pc *= f;
+  pm *= f;
+}
+
+// 2a. Bracket [lo, hi] of the lowest eigenvalue of T, T - lo I positive
+// definite; warps [0, kEigBracketWarps).  Returns lo and hi in every thread.
+__device__ __forceinline__ void eig_bracket(int n, const EigVecs& V, double& lo_out, double& hi_out) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  constexpr int T = 32 * kEigBracketWarps;
+  __shared__ int s_first[2][kEigBracketWarps];
+  __shared__ double s_lohi[2];
+  const double* const d = V.d;
+  double* const e2 = V.e2;
   if (warp == 0) {
     double lo = 1e300, hi = -1e300;
     for (int i = lane; i < n; i += 32) {
-      const double em = (i > 0) ? fabs(ws.e[i - 1]) : 0.0;
-      const double ep = (i < n - 1) ? fabs(ws.e[i]) : 0.0;
-      lo = fmin(lo, ws.d[i] - em - ep);
-      hi = fmax(hi, ws.d[i] + em + ep);
-      if (i < n - 1) ws.e2[i] = ws.e[i] * ws.e[i];
+      const double em = (i > 0) ? fabs(V.e[i - 1]) : 0.0;
+      const double ep = (i < n - 1) ? fabs(V.e[i]) : 0.0;
+      lo = fmin(lo, d[i] - em - ep);
+      hi = fmax(hi, d[i] + em + ep);
+      if (i < n - 1) e2[i] = V.e[i] * V.e[i];
     }
     for (int o = 16; o > 0; o >>= 1) {
       lo = fmin(lo, __shfl_xor_sync(~0u, lo, o));
@@ -152,123 +274,271 @@ __device__ void smallest_eigvec(EigScratch& ws, int n, SectionClock& clk) {
     }
     if (lane == 0) {
       const double widen = 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300;
-      ws.scal[2] = lo - widen;
-      ws.scal[3] = hi + widen;
+      s_lohi[0] = lo - widen;
+      s_lohi[1] = hi + widen;
     }
   }
-  __syncthreads();
-  for (int round = 0; round < 4; ++round) {
-    const double lo = ws.scal[2], hi = ws.scal[3];
-    if (tid == 0) *ws.ibest = NT;
-    __syncthreads();
-    const double sig = lo + (hi - lo) * (static_cast<double>(tid + 1) / static_cast<double>(NT + 1));
-    // Sign changes in p_0 = 1, p_1 = d_0 - sig, p_i = (d_{i-1} - sig) p_{i-1} - e_{i-2}^2 p_{i-2};
-    // a zero takes the sign opposite to its predecessor.
-    double pm = 1.0, pc = ws.d[0] - sig;
-    int sprev = 1, cnt = 0;
-    int sc = (pc > 0.0) ? 1 : (pc < 0.0 ? -1 : -sprev);
-    cnt += (sc != sprev);
-    sprev = sc;
-    for (int i = 1; i < n; ++i) {
-      const double pn = (ws.d[i] - sig) * pc - ws.e2[i - 1] * pm;
+  bar_named(2, T);
+  double lo = s_lohi[0], hi = s_lohi[1];
+  const double inv = 1.0 / static_cast<double>(T + 1);
+  for (int round = 0; round < kEigBracketRounds; ++round) {
+    const double w = hi - lo;
+    const double sig = fma(w, static_cast<double>(t + 1) * inv, lo);
+    // Not positive definite at sig <=> some leading minor <= 0.  No early
+    // exit: the loop stays free of data-dependent branches.
+    double pm = 1.0, pc = d[0] - sig;
+    bool neg = !(pc > 0.0);
+    int i = 1;
+    for (; i + 3 < n; i += 4) {
+      double di[4], ei[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        di[q] = d[i + q];
+        ei[q] = e2[i + q - 1];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double pn = fma(di[q] - sig, pc, -ei[q] * pm);
+        pm = pc;
+        pc = pn;
+        neg |= !(pc > 0.0);
+      }
+      pair_rescale(pc, pm);
+    }
+    for (; i < n; ++i) {
+      const double pn = fma(d[i] - sig, pc, -e2[i - 1] * pm);
       pm = pc;
       pc = pn;
-      const double big = fabs(pc) + fabs(pm);
-      if (big > 1e150 || (big < 1e-150 && big > 0.0)) {
-        const double f = big > 1e150 ? 0x1p-500 : 0x1p+500;
-        pc *= f;
-        pm *= f;
-      }
-      sc = (pc > 0.0) ? 1 : (pc < 0.0 ? -1 : -sprev);
-      cnt += (sc != sprev);
-      sprev = sc;
+      neg |= !(pc > 0.0);
     }
-    if (cnt >= 1) atomicMin(ws.ibest, tid);
-    __syncthreads();
-    if (tid == 0) {
-      const int t = *ws.ibest;
-      if (t < NT) {
-        ws.scal[3] = lo + (hi - lo) * (static_cast<double>(t + 1) / static_cast<double>(NT + 1));
-        if (t > 0) ws.scal[2] = lo + (hi - lo) * (static_cast<double>(t) / static_cast<double>(NT + 1));
-      } else {
-        ws.scal[2] = lo + (hi - lo) * (static_cast<double>(NT) / static_cast<double>(NT + 1));
-      }
+    const unsigned b = __ballot_sync(~0u, neg);
+    if (lane == 0) s_first[round & 1][warp] = b ? warp * 32 + __ffs(b) - 1 : T;
+    bar_named(2, T);
+    int f = T;
+    for (int q = 0; q < kEigBracketWarps; ++q) f = min(f, s_first[round & 1][q]);
+    if (f < T) {
+      const double nlo = f > 0 ? fma(w, static_cast<double>(f) * inv, lo) : lo;
+      hi = fma(w, static_cast<double>(f + 1) * inv, lo);
+      lo = nlo;
+    } else {
+      lo = fma(w, static_cast<double>(T) * inv, lo);
     }
-    __syncthreads();
   }
-  clk.mark(11);
+  lo_out = lo;
+  hi_out = hi;
+}
 
-  // 3. Inverse iteration on T - sigma I (thread 0; 1/u and l reuse hv and p).
-  if (tid == 0) {
-    const double sigma = ws.scal[2];
-    const double tiny = 1e-290;
-    double* ru = ws.hv;
-    double* l = ws.p;
-    double u = ws.d[0] - sigma;
-    if (fabs(u) < tiny) u = tiny;
-    ru[0] = 1.0 / u;
-    for (int i = 1; i < n; ++i) {
-      const double li = ws.e[i - 1] * ru[i - 1];
-      l[i] = li;
-      u = (ws.d[i] - sigma) - li * ws.e[i - 1];
-      if (fabs(u) < tiny) u = tiny;
-      ru[i] = 1.0 / u;
+// 2b. M[i][j] = tau_i u_j^T u_i for 0 <= j < i <= n-3 into A[i][j]; threads
+// [t0, t0 + nthreads).
+__device__ __forceinline__ void eig_gram(double* A, int lda, int n, const EigVecs& V, int t0, int nthreads) {
+  const int nr = n - 2;
+  const int P = nr > 1 ? nr * (nr - 1) / 2 : 0;
+  for (int idx = static_cast<int>(threadIdx.x) - t0; idx < P; idx += nthreads) {
+    int i = static_cast<int>((1.0f + sqrtf(1.0f + 8.0f * static_cast<float>(idx))) * 0.5f);
+    while (i * (i - 1) / 2 > idx) --i;
+    while (i * (i + 1) / 2 <= idx) ++i;
+    const int j = idx - i * (i - 1) / 2;
+    const double* ri = A + i * lda;
+    const double* rj = A + j * lda;
+    double s0 = rj[i + 1] * V.u0[i], s1 = 0.0;
+    int c = i + 2;
+    for (; c + 1 < n; c += 2) {
+      s0 = fma(rj[c], ri[c], s0);
+      s1 = fma(rj[c + 1], ri[c + 1], s1);
     }
-    double* y = ws.y;
-    for (int i = 0; i < n; ++i) y[i] = 1.0 + 0.0625 * static_cast<double>((7 * i + 3) % 11);
+    if (c < n) s0 = fma(rj[c], ri[c], s0);
+    A[i * lda + j] = V.tau[i] * (s0 + s1);
+  }
+}
+
+// 3. Three steps of inverse iteration on T - sigma I from a fixed start
+// vector; warp 0.  Writes V.y (scaled down whenever its largest element
+// passes 1e100).
+__device__ __forceinline__ void eig_inverse_iteration(int n, const EigVecs& V, double sigma) {
+  const int lane = threadIdx.x & 31;
+  const double* const d = V.d;
+  const double* const e = V.e;
+  const double* const e2 = V.e2;
+  double* const num = V.num;
+  double* const den = V.den;
+  double* const ru = V.ru;
+  double* const l = V.l;
+  double* const y = V.y;
+  for (int i = lane; i < n; i += 32) y[i] = 1.0 + 0.0625 * static_cast<double>((7 * i + 3) % 11);
+  if (lane == 0) {
+    double pm = 1.0, pc = d[0] - sigma;
+    num[0] = pc;
+    den[0] = 1.0;
+    int i = 1;
+    for (; i + 3 < n; i += 4) {
+      double di[4], ei[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        di[q] = d[i + q];
+        ei[q] = e2[i + q - 1];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double pn = fma(di[q] - sigma, pc, -ei[q] * pm);
+        num[i + q] = pn;
+        den[i + q] = pc;
+        pm = pc;
+        pc = pn;
+      }
+      pair_rescale(pc, pm);
+    }
+    for (; i < n; ++i) {
+      const double pn = fma(d[i] - sigma, pc, -e2[i - 1] * pm);
+      num[i] = pn;
+      den[i] = pc;
+      pm = pc;
+      pc = pn;
+    }
+  }
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) {
+    double u = num[i] / den[i];
+    if (!(fabs(u) >= 1e-290)) u = 1e-290;  // also catches a NaN pivot
+    ru[i] = 1.0 / u;
+  }
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) l[i] = i > 0 ? e[i - 1] * ru[i - 1] : 0.0;
+  __syncwarp();
+  if (lane == 0) {
     for (int it = 0; it < 3; ++it) {
+      // L z = y: z_i = y_i - l_i z_{i-1}, in chunks of four (loads first).
       double prev = y[0];
-      for (int i = 1; i < n; ++i) {
-        prev = y[i] - l[i] * prev;
+      int i = 1;
+      for (; i + 3 < n; i += 4) {
+        double li[4], yi[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          li[q] = l[i + q];
+          yi[q] = y[i + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          prev = fma(-li[q], prev, yi[q]);
+          y[i + q] = prev;
+        }
+      }
+      for (; i < n; ++i) {
+        prev = fma(-l[i], prev, y[i]);
         y[i] = prev;
       }
+      // U y = z: y_i = (z_i - e_i y_{i+1}) / u_i.
       double next = y[n - 1] * ru[n - 1];
       y[n - 1] = next;
       double mx = fabs(next);
-      for (int i = n - 2; i >= 0; --i) {
-        next = (y[i] - ws.e[i] * next) * ru[i];
+      i = n - 2;
+      for (; i >= 3; i -= 4) {
+        double ei[4], zi[4], ri[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ei[q] = e[i - q];
+          zi[q] = y[i - q];
+          ri[q] = ru[i - q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          next = fma(-ei[q], next, zi[q]) * ri[q];
+          y[i - q] = next;
+          mx = fmax(mx, fabs(next));
+        }
+      }
+      for (; i >= 0; --i) {
+        next = fma(-e[i], next, y[i]) * ru[i];
         y[i] = next;
         mx = fmax(mx, fabs(next));
       }
-      const double inv = mx > 0.0 ? 1.0 / mx : 1.0;
-      for (int i = 0; i < n; ++i) y[i] *= inv;
+      if (mx > 1e100)
+        for (int q = 0; q < n; ++q) y[q] *= 1e-100;
+    }
+  }
+  __syncwarp();
+}
+
+// Block-wide.  On return V.y[0..n) holds an (unnormalised) eigenvector of the
+// lowest eigenvalue of the matrix originally in A (n x n, leading dimension
+// lda, both triangles); A is overwritten.  clk marks sections 10..12.
+__device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigVecs& V, SectionClock& clk) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (n == 1) {
+    if (tid == 0) V.y[0] = 1.0;
+    __syncthreads();
+    return;
+  }
+  const int nwa = (n - 1 + 31) / 32;
+  if (warp < nwa) eig_tridiag(A, lda, n, V, nwa);
+  __syncthreads();
+  clk.mark(10);
+
+  if (warp < kEigBracketWarps) {
+    double lo, hi;
+    eig_bracket(n, V, lo, hi);
+    clk.mark(11);
+    if (warp == 0) eig_inverse_iteration(n, V, lo);
+    clk.mark(12);
+  } else {
+    eig_gram(A, lda, n, V, 32 * kEigBracketWarps, static_cast<int>(blockDim.x) - 32 * kEigBracketWarps);
+  }
+  __syncthreads();
+
+  // 4. Back-transformation.
+  double* y = V.y;
+  for (int j = warp; j < n - 2; j += 32) {
+    const double* rj = A + j * lda;
+    double s = 0.0;
+    for (int c = j + 2 + lane; c < n; c += 32) s = fma(rj[c], y[c], s);
+    s = warp_sum(s);
+    if (lane == 0) V.c[j] = fma(V.u0[j], y[j + 1], s);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int Q = (kMaxK + 1 + 31) / 32;
+    double tq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int j = lane + 32 * q;
+      tq[q] = j < n - 2 ? V.c[j] : 0.0;
+    }
+    double mrow[Q];  // M[i][lane + 32q], loaded one step ahead
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int j = lane + 32 * q;
+      mrow[q] = (n >= 3 && j < n - 3) ? A[(n - 3) * lda + j] : 0.0;
+    }
+    for (int i = n - 3; i >= 0; --i) {
+      double mnext[Q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int j = lane + 32 * q;
+        mnext[q] = (i >= 1 && j < i - 1) ? A[(i - 1) * lda + j] : 0.0;
+      }
+      const int qi = i >> 5;
+      double own = tq[0];
+#pragma unroll
+      for (int q = 1; q < Q; ++q) own = (qi == q) ? tq[q] : own;
+      const double si = __shfl_sync(~0u, own, i & 31);
+      if (lane == (i & 31)) V.g[i] = V.tau[i] * si;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int j = lane + 32 * q;
+        if (j < i) tq[q] = fma(-mrow[q], si, tq[q]);
+        mrow[q] = mnext[q];
+      }
     }
   }
   __syncthreads();
-  clk.mark(12);
-
-  // 4. Back-transformation y <- H_0 ... H_{n-3} y (warp 0, y in registers:
-  //    lane holds y[lane + 32q]).
-  if (warp == 0) {
-    constexpr int QY = (kMaxK + 1 + 31) / 32;
-    double yr[QY];
-#pragma unroll
-    for (int q = 0; q < QY; ++q) {
-      const int t = lane + 32 * q;
-      yr[q] = t < n ? ws.y[t] : 0.0;
+  for (int r = warp; r < n; r += 32) {
+    const int jmax = min(r - 1, n - 3);
+    double s = 0.0;
+    for (int j = lane; j <= jmax; j += 32) {
+      const double ujr = (j == r - 1) ? V.u0[j] : A[j * lda + r];
+      s = fma(V.g[j], ujr, s);
     }
-    for (int j = n - 3; j >= 0; --j) {
-      const double bet = ws.beta[j];
-      if (bet == 0.0) continue;
-      const double* hvj = A + j * lda;  // v_j[i] at hvj[j + 1 + i]
-      double s = 0.0;
-#pragma unroll
-      for (int q = 0; q < QY; ++q) {
-        const int t = lane + 32 * q;
-        if (t > j && t < n) s = fma(hvj[t], yr[q], s);
-      }
-      s = __shfl_sync(~0u, warp_sum(s), 0) * bet;
-#pragma unroll
-      for (int q = 0; q < QY; ++q) {
-        const int t = lane + 32 * q;
-        if (t > j && t < n) yr[q] -= s * hvj[t];
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < QY; ++q) {
-      const int t = lane + 32 * q;
-      if (t < n) ws.y[t] = yr[q];
-    }
+    s = warp_sum(s);
+    if (lane == 0) y[r] -= s;
   }
   __syncthreads();
 }

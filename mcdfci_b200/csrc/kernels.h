@@ -124,9 +124,10 @@ cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, 
                          double* v_out, int cap, int* n_out, cudaStream_t s);
 cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cudaStream_t s);
 // One eig update on given inputs (device pointers); writes dx[k], xx_scale[0] =
-// new xx, xx_scale[1] = new scale, the branch taken and an error word.
-cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
-                      double* dx, dd* xx_scale, int* branch, unsigned* err, cudaStream_t s);
+// new xx, xx_scale[1] = new scale, the branch taken and an error word.  The
+// lower triangle of hsub is overwritten with its upper triangle.
+cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
+                      dd* xx_scale, int* branch, unsigned* err, cudaStream_t s);
 size_t leader_smem_bytes(int k, int m);
 
 // debug_eig on HOST buffers with its device buffers in a file-scope device

@@ -146,8 +146,10 @@ __device__ __forceinline__ double score_of(double x, double z, dd xss) {
 
 // ---------------------------------------------------------------------------
 // Eig update.  Inputs x[k], z[k] in shared memory; H (row-major k x k,
-// symmetric) in shared or global memory; `work` is shared scratch of
-// eig_work_doubles(k) doubles.  Outputs dx[k] (shared), new xx and scale.
+// symmetric: dsyevr with UPLO='L' on the row-major array reads its upper
+// triangle, and callers fill the lower one from it) in shared or global
+// memory; `work` is shared scratch of eig_work_doubles(k) doubles.  Outputs
+// dx[k] (shared), new xx and scale.
 
 struct EigResult {
   dd xx, scale;
@@ -156,28 +158,62 @@ struct EigResult {
   double resid;
 };
 
+constexpr int kEigVecs = 18;
+
 __host__ __device__ constexpr size_t eig_work_doubles(int k) {
-  return static_cast<size_t>(k + 1) * (k + 1) + 12 * static_cast<size_t>(k + 1) + 64;
+  return static_cast<size_t>(k + 1) * eig_lda(k + 1) + kEigVecs * static_cast<size_t>(k + 1) + 64;
 }
 
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
                                 double* dx, double* work, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ double s_b00, s_y1;
-  __shared__ dd s_red[32];
-  __shared__ double s_redd[32];
+  __shared__ double s_b00, s_y1, s_res;
   __shared__ int s_branch;
-  __shared__ int s_ibest;
   __shared__ dd s_rq;
   EigResult res;
 
-  // x'x, x'z, Hx, x'Hx in double-double, rounded where the reference works in double.
-  double* Hx = work;  // [k]
+  // B = [[b00, b'], [b, H]] in A (leading dimension lda); H's block at (1, 1)
+  // also serves the first-iteration k x k problem.
+  const int lda = eig_lda(k + 1);
+  double* A = work;
+  double* vec = work + static_cast<size_t>(k + 1) * lda;
+  const int vs = k + 1;
+  EigVecs V;
+  V.d = vec;
+  V.e = vec + vs;
+  V.e2 = vec + 2 * vs;
+  V.u0 = vec + 3 * vs;
+  V.tau = vec + 4 * vs;
+  V.num = vec + 5 * vs;
+  V.den = vec + 6 * vs;
+  V.ru = vec + 7 * vs;
+  V.l = vec + 8 * vs;
+  V.y = vec + 9 * vs;
+  V.c = vec + 10 * vs;
+  V.g = vec + 11 * vs;
+  double* Hx = vec + 12 * vs;    // [k]
+  double* bvec = vec + 13 * vs;  // [k+1] first row of B (branch 1)
+  double* Bv = vec + 14 * vs;
+  double* vhi = vec + 15 * vs;   // normalised eigenvector, hi part
+  double* vlo = vec + 16 * vs;   // lo part
+
+  for (int idx = tid; idx < k * k; idx += blockDim.x) {
+    const int i = idx / k, j = idx - i * k;
+    if (i <= j) {
+      const double v = H[idx];
+      A[(i + 1) * lda + (j + 1)] = v;
+      A[(j + 1) * lda + (i + 1)] = v;
+    }
+  }
+  __syncthreads();
+  // H x in double (dsymv, src/solver.h:355); x'x, x'z, x'Hx in double-double,
+  // rounded where the reference works in double.
   for (int r = warp; r < k; r += 32) {
-    dd s{0.0, 0.0};
-    for (int c = lane; c < k; c += 32) s = dd_add(s, dd_two_prod(H[r * k + c], x[c]));
-    s = warp_sum_dd(s);
-    if (lane == 0) Hx[r] = dd_to_d(s);
+    const double* row = A + (r + 1) * lda + 1;
+    double s = 0.0;
+    for (int c = lane; c < k; c += 32) s = fma(row[c], x[c], s);
+    s = warp_sum(s);
+    if (lane == 0) Hx[r] = s;
   }
   __syncthreads();
   if (warp == 0) {
@@ -205,117 +241,77 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   __syncthreads();
   const int branch = s_branch;
   const int n = branch == 1 ? k + 1 : k;
-  const int off = branch == 1 ? 1 : 0;
   const double y1 = s_y1;
-
-  double* base = work + ((k + 1) & ~1) + 2;
-  EigScratch ws;
-  ws.lda = n;
-  ws.A = base;
-  ws.d = ws.A + static_cast<size_t>(n) * n;
-  ws.e = ws.d + n;
-  ws.e2 = ws.e + n;
-  ws.beta = ws.e2 + n;
-  ws.hv = ws.beta + n;
-  ws.p = ws.hv + n;
-  ws.y = ws.p + n;
-  double* bvec = ws.y + n;   // [n] first row of B (branch 1)
-  double* vhi = bvec + n;    // [n] normalised eigenvector, hi part
-  double* vlo = vhi + n;     // [n] lo part
-  ws.part = vlo + n;         // [32]
-  ws.scal = ws.part + 32;    // [8]
-  ws.ibest = &s_ibest;
-
-  // B = [[b00, b'], [b, H]] with b = (z - Hx) / y1; only the upper triangle of
-  // H is used, as dsyevr with UPLO='L' on the row-major array does.
-  for (int idx = tid; idx < n * n; idx += blockDim.x) {
-    const int r = idx / n, c = idx - r * n;
-    double v;
-    if (r >= off && c >= off) {
-      const int i = r - off, j = c - off;
-      v = (i <= j) ? H[i * k + j] : H[j * k + i];
-    } else if (r == 0 && c == 0) {
-      v = s_b00;
-    } else {
-      const int i = (r == 0 ? c : r) - 1;
-      v = (z[i] - Hx[i]) / y1;
+  if (branch == 1) {
+    // b = (z - Hx) / y1 (src/solver.h:378-383).
+    for (int i = tid; i <= k; i += blockDim.x) {
+      const double v = i == 0 ? s_b00 : (z[i - 1] - Hx[i - 1]) / y1;
+      A[i] = v;
+      A[i * lda] = v;
+      bvec[i] = v;
     }
-    ws.A[idx] = v;
-    if (r == 0) bvec[c] = v;
   }
   __syncthreads();
   clk.mark(9);
 
-  smallest_eigvec(ws, n, clk);
+  double* Ae = branch == 1 ? A : A + lda + 1;
+  eig_lowest(Ae, lda, n, V, clk);
   clk.mark(13);
 
-  // Normalise in double-double; fix the sign.
+  // B v in double, one row per warp (H is symmetric, so its rows are read).
+  const double* y = V.y;
+  for (int r = warp; r < n; r += 32) {
+    double s = 0.0;
+    if (branch == 1) {
+      const double* hr = H + (r - 1) * k - 1;  // hr[c] = H[r-1][c-1]
+      for (int c = lane; c < n; c += 32) {
+        const double brc = (r == 0) ? bvec[c] : (c == 0 ? bvec[r] : hr[c]);
+        s = fma(brc, y[c], s);
+      }
+    } else {
+      const double* hr = H + r * k;
+      for (int c = lane; c < n; c += 32) s = fma(hr[c], y[c], s);
+    }
+    s = warp_sum(s);
+    if (lane == 0) Bv[r] = s;
+  }
+  __syncthreads();
+  // Rayleigh quotient y'By / y'y, normalisation in double-double, sign fix,
+  // residual ||B v - lambda v||.
   if (warp == 0) {
-    dd nrm{0, 0};
+    dd nrm{0, 0}, num{0, 0};
     double sgn = 0.0;
     for (int i = lane; i < n; i += 32) {
-      nrm = dd_add(nrm, dd_two_prod(ws.y[i], ws.y[i]));
-      if (branch == 2) sgn += ws.y[i] * x[i];
+      nrm = dd_add(nrm, dd_two_prod(y[i], y[i]));
+      num = dd_add(num, dd_two_prod(y[i], Bv[i]));
+      if (branch == 2) sgn = fma(y[i], x[i], sgn);
     }
     nrm = warp_sum_dd(nrm);
+    num = warp_sum_dd(num);
     sgn = warp_sum(sgn);
-    nrm = dd{__shfl_sync(~0u, nrm.hi, 0), __shfl_sync(~0u, nrm.lo, 0)};
-    sgn = __shfl_sync(~0u, sgn, 0);
-    const double flip = (branch == 1) ? (ws.y[0] < 0.0 ? -1.0 : 1.0) : (sgn < 0.0 ? -1.0 : 1.0);
+    const dd rq = dd_div(num, nrm);
+    const double lam = dd_to_d(rq);
+    const double flip = (branch == 1) ? (y[0] < 0.0 ? -1.0 : 1.0) : (sgn < 0.0 ? -1.0 : 1.0);
     const dd inv = dd_div(dd{flip, 0.0}, dd_sqrt(nrm));
+    double acc = 0.0;
     for (int i = lane; i < n; i += 32) {
-      const dd vi = dd_mul_d(inv, ws.y[i]);
+      const dd vi = dd_mul_d(inv, y[i]);
       vhi[i] = vi.hi;
       vlo[i] = vi.lo;
-    }
-  }
-  __syncthreads();
-
-  // Rayleigh quotient v'Bv in double-double, and B v in double for the residual.
-  {
-    dd acc{0, 0};
-    for (int r = warp; r < n; r += 32) {
-      dd s{0, 0};
-      double sd = 0.0;
-      for (int c = lane; c < n; c += 32) {
-        double brc;
-        if (r >= off && c >= off) {
-          const int i = r - off, j = c - off;
-          brc = (i <= j) ? H[i * k + j] : H[j * k + i];
-        } else {
-          brc = bvec[r == 0 ? c : r];
-        }
-        s = dd_add(s, dd_mul_d(dd{vhi[c], vlo[c]}, brc));
-        sd += brc * vhi[c];
-      }
-      s = warp_sum_dd(s);
-      s = dd{__shfl_sync(~0u, s.hi, 0), __shfl_sync(~0u, s.lo, 0)};
-      sd = __shfl_sync(~0u, warp_sum(sd), 0);
-      acc = dd_add(acc, dd_mul(s, dd{vhi[r], vlo[r]}));
-      if (lane == 0) ws.hv[r] = sd;  // (B v)_r for the residual
-    }
-    if (lane == 0) s_red[warp] = acc;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    const dd t = warp_sum_dd(lane < static_cast<int>(blockDim.x >> 5) ? s_red[lane] : dd{0.0, 0.0});
-    if (lane == 0) s_rq = t;
-  }
-  __syncthreads();
-  const dd rq = s_rq;
-  const double lam = dd_to_d(rq);
-  if (warp == 0) {
-    double acc = 0.0;
-    for (int r = lane; r < n; r += 32) {
-      const double t = ws.hv[r] - lam * vhi[r];
-      acc += t * t;
+      const double t = fma(-lam, y[i], Bv[i]);
+      acc = fma(t, t, acc);
     }
     acc = warp_sum(acc);
-    if (lane == 0) s_redd[0] = acc;
+    if (lane == 0) {
+      s_rq = rq;
+      s_res = sqrt(acc / dd_to_d(nrm));
+    }
   }
   __syncthreads();
   clk.mark(14);
-  res.resid = sqrt(s_redd[0]);
+  const dd rq = s_rq;
+  const double lam = dd_to_d(rq);
+  res.resid = s_res;
   res.branch = branch;
   res.ok = true;
 
@@ -349,7 +345,6 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
 }
 
 // ---------------------------------------------------------------------------
-
 // End of iteration t (src/wavefunction.h:557-565,583): z[D_c] = new_z_c for
 // the picked determinants, then xz += sum_c dot_c.  Block-wide, on a state
 // copy `S` (shared or global); table stores go to global memory.
@@ -780,16 +775,26 @@ __global__ void debug_hsub_kernel(HamDev h, const Det* dets, int k, double* H) {
   }
 }
 
-__global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, const double* H, const double* x,
-                                                           const double* z, dd xx, dd xz, double* dx,
-                                                           dd* out, int* branch, unsigned* err) {
+// Lower triangle of the row-major k x k matrix H := its upper triangle (the
+// part of H_sub the reference's dsyevr/dsymv calls read); block-wide.
+__device__ void symmetrise_from_upper(double* H, int k) {
+  for (int idx = threadIdx.x; idx < k * k; idx += blockDim.x) {
+    const int i = idx / k, j = idx - i * k;
+    if (i < j) H[j * k + i] = H[idx];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, const double* x, const double* z,
+                                                           dd xx, dd xz, double* dx, dd* out, int* branch,
+                                                           unsigned* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
   for (int i = threadIdx.x; i < k; i += blockDim.x) {
     s_x[i] = x[i];
     s_z[i] = z[i];
   }
-  __syncthreads();
+  symmetrise_from_upper(H, k);
   SectionClock clk{nullptr, 0};
   const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
   for (int i = threadIdx.x; i < k; i += blockDim.x) dx[i] = s_dx[i];
@@ -842,8 +847,8 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
   return cudaGetLastError();
 }
 
-cudaError_t debug_eig(int k, const double* hsub, const double* x, const double* z, dd xx, dd xz,
-                      double* dx, dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
+cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
+                      dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
   const size_t bytes = eig_work_doubles(k) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(debug_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(bytes));
@@ -882,7 +887,7 @@ __global__ void __launch_bounds__(kLT, 1) static_eig_kernel(int k, double* base,
     s_x[i] = base[kStaticEigX + i];
     s_z[i] = base[kStaticEigZ + i];
   }
-  __syncthreads();
+  symmetrise_from_upper(base + kStaticEigH, k);
   SectionClock clk{nullptr, 0};
   const EigResult er = eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
   for (int i = threadIdx.x; i < k; i += blockDim.x) base[kStaticEigDx + i] = s_dx[i];

@@ -5,12 +5,12 @@
 // step of __float128 inverse iteration through dgetrf (src/solver.h:400-503).
 // Here the work is arranged around the serial dependencies of one CTA:
 //   1. Householder reduction to tridiagonal T = Q^T A Q (Golub & Van Loan,
-//      Algorithm 8.3.1) by the first ceil((n-1)/32) warps, one pass over the
-//      trailing rows per step: the next pivot row is updated first, one
-//      column per thread, every thread derives the next reflector from two
-//      sums, and then each thread updates its own row with reflector j while
-//      forming its element of p = tau A u for reflector j+1.  Reflector j is
-//      H_j = I - tau_j u_j u_j^T with u_j = (0..0, A[j][j+1..n)), where
+//      Algorithm 8.3.1) by four warps per 32 rows, one pass over the trailing
+//      rows per step: the next pivot row is updated first, one column per
+//      thread, every thread derives the next reflector from its norm, and
+//      then the trailing rows, each split over four lanes, are updated with
+//      reflector j while p = tau A u for reflector j+1 is formed.  Reflector
+//      j is H_j = I - tau_j u_j u_j^T with u_j = (0..0, A[j][j+1..n)), where
 //      A[j][j+1] holds u0_j; row j is not written after step j.
 //   2. The lowest eigenvalue of T is bracketed by 128-way multisection on four
 //      warps (one per SM sub-partition): T - sigma I is positive definite
@@ -73,45 +73,34 @@ __device__ __forceinline__ void eig_reflector(double x0, double s, double& u0, d
   e = -sg * mu;
 }
 
-// 1. Tridiagonalisation; threads [0, 32*nwa) only, 32*nwa >= n-1, n >= 2.
+// Warps taking part in the reduction of an n x n matrix: four per 32
+// trailing rows, so that each row is split over four lanes.
+__host__ __device__ constexpr int eig_tridiag_warps(int n) { return 4 * ((n - 1 + 31) / 32); }
+
+// 1. Tridiagonalisation; threads [0, 32*eig_tridiag_warps(n)) only, n >= 2.
 // Step j, with reflector j, p = tau_j A u_j and K = tau_j/2 p'u_j known:
-//   (a) w = p - K u_j, one column per thread;
-//   (b) row j+1 after the update, one column per thread: its diagonal is
-//       d_{j+1}, the rest defines reflector j+1, whose scalars every thread
-//       derives from two sums;
-//   (c) rows j+2.. after the update, one row per thread, in the same pass as
-//       p = tau_{j+1} A u_{j+1}.
-// A[j][j+1] is replaced by u0_j, so u_j is row j from column j+1 on.
-__device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const EigVecs& V, int nwa) {
+//   (a) row j+1 after the update, one column per thread (w = p - K u_j on
+//       the fly): its diagonal is d_{j+1}, the rest defines reflector j+1,
+//       whose scalars every thread derives from its squared norm and first
+//       element;
+//   (b) rows j+2.. after the update, each row split over four lanes
+//       (interleaved columns), in the same pass as p = tau_{j+1} A u_{j+1}.
+// A[j][j+1] is replaced by u0_j, so u_j is row j from column j+1 on.  Each
+// lane of a single warp issues only about one shared-memory access per ten
+// cycles, so the row pass is spread over four warps per 32 rows, one per SM
+// sub-partition, and w and the row scalars go through shared memory rather
+// than shuffles.
+__device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const EigVecs& V) {
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const int T = 32 * nwa;
+  const int nwc = (n - 1 + 31) / 32;  // warps holding the column owners
+  const int T = 32 * 4 * nwc;
+  const int rs = wid * 8 + (lane & 7);  // row slot of this thread
+  const int seg = lane >> 3;            // its quarter of the row
   double* const P = V.num;
   double* const W = V.den;
-  __shared__ double s_red[2][kEigBracketWarps][2];
-  // Sums of a and b over the participating threads, identical in all of them.
-  auto sum2 = [&](double& a, double& b, int buf) {
-    a = warp_sum(a);
-    b = warp_sum(b);
-    if (nwa > 1) {
-      if (lane == 0) {
-        s_red[buf][wid][0] = a;
-        s_red[buf][wid][1] = b;
-      }
-      bar_named(1, T);
-      a = 0.0;
-      b = 0.0;
-      for (int q = 0; q < nwa; ++q) {
-        a += s_red[buf][q][0];
-        b += s_red[buf][q][1];
-      }
-    }
-  };
-  auto sync = [&]() {
-    if (nwa == 1)
-      __syncwarp();
-    else
-      bar_named(1, T);
-  };
+  __shared__ double s_part[2][4];
+  __shared__ double s_x0[2];
+  __shared__ double s_kp[2][16];
   if (n == 2) {
     if (t == 0) {
       V.d[0] = A[0];
@@ -120,17 +109,37 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
     }
     return;
   }
+  // Sum over the four lanes of a row, then over the rows of the warp, of a
+  // value held by segment 0; partial per warp into s_kp[buf][wid].
+  auto kp_partial = [&](double v, int buf) {
+    v = warp_sum(v);
+    if (lane == 0) s_kp[buf][wid] = v;
+  };
+  auto kp_total = [&](int buf) {
+    double k = 0.0;
+    for (int q = 0; q < T / 32; ++q) k += s_kp[buf][q];
+    return k;
+  };
 
-  // Reflector 0 from row 0; p and K of step 0.
+  // Reflector 0 from row 0.
   double tau, K;
   {
     const int c = 1 + t;
-    const double a = c < n ? A[c] : 0.0;
-    double sq = (c >= 2 && c < n) ? a * a : 0.0;
-    double x0 = (c == 1) ? a : 0.0;
-    sum2(sq, x0, 0);
+    double sq = 0.0;
+    if (c < n) {
+      const double a = A[c];
+      if (c >= 2) sq = a * a;
+      if (c == 1) s_x0[0] = a;
+    }
+    if (wid < nwc) {
+      sq = warp_sum(sq);
+      if (lane == 0) s_part[0][wid] = sq;
+    }
+    bar_named(1, T);
+    sq = 0.0;
+    for (int q = 0; q < nwc; ++q) sq += s_part[0][q];
     double u0, e0;
-    eig_reflector(x0, sq, u0, tau, e0);
+    eig_reflector(s_x0[0], sq, u0, tau, e0);
     if (t == 0) {
       V.d[0] = A[0];
       V.e[0] = e0;
@@ -138,52 +147,63 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
       V.tau[0] = tau;
       A[1] = u0;
     }
-    sync();
-    const int r = 1 + t;
-    double p = 0.0, ur = 0.0;
+    bar_named(1, T);
+    // p for reflector 0.
+    const int r = 1 + rs;
+    double p = 0.0;
     if (r < n) {
       const double* Rr = A + r * lda;
-      double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
-      int cc = 1;
-      for (; cc + 3 < n; cc += 4) {
+      double p0 = 0.0, p1 = 0.0;
+      int cc = 1 + seg;
+      for (; cc + 4 < n; cc += 8) {
         p0 = fma(Rr[cc], A[cc], p0);
-        p1 = fma(Rr[cc + 1], A[cc + 1], p1);
-        p2 = fma(Rr[cc + 2], A[cc + 2], p2);
-        p3 = fma(Rr[cc + 3], A[cc + 3], p3);
+        p1 = fma(Rr[cc + 4], A[cc + 4], p1);
       }
-      for (; cc < n; ++cc) p0 = fma(Rr[cc], A[cc], p0);
-      p = tau * ((p0 + p1) + (p2 + p3));
-      ur = A[r];
-      P[r] = p;
+      if (cc < n) p0 = fma(Rr[cc], A[cc], p0);
+      p = p0 + p1;
     }
-    double kp = p * ur, zero = 0.0;
-    sum2(kp, zero, 1);
-    K = 0.5 * tau * kp;
+    p += __shfl_xor_sync(~0u, p, 8);
+    p += __shfl_xor_sync(~0u, p, 16);
+    p *= tau;
+    double kp = 0.0;
+    if (r < n && seg == 0) {
+      P[r] = p;
+      kp = p * A[r];
+    }
+    kp_partial(kp, 0);
+    bar_named(1, T);
+    K = 0.5 * tau * kp_total(0);
   }
 
   for (int j = 0; j + 2 < n; ++j) {
+    const int buf = j & 1;
     const double* Uj = A + j * lda;  // u_j from column j+1
     double* R1 = A + (j + 1) * lda;  // the next pivot row
     const bool more = j + 3 < n;     // reflector j+1 exists
     // (a)
     const int c = j + 1 + t;
-    double uc = 0.0, wc = 0.0;
+    double a = 0.0, sq = 0.0;
     if (c < n) {
-      uc = Uj[c];
-      wc = fma(-K, uc, P[c]);
+      const double uc = Uj[c];
+      const double wc = fma(-K, uc, P[c]);
       W[c] = wc;
+      const double u1 = Uj[j + 1];
+      const double w1 = fma(-K, u1, P[j + 1]);
+      a = fma(-u1, wc, fma(-w1, uc, R1[c]));
+      if (c >= j + 3) sq = a * a;
+      if (c == j + 2) s_x0[buf] = a;
+      if (c == j + 1) V.d[j + 1] = a;
     }
-    sync();
-    // (b)
-    const double u1 = Uj[j + 1], w1 = W[j + 1];
-    double a = 0.0;
-    if (c < n) a = fma(-u1, wc, fma(-w1, uc, R1[c]));
-    double sq = (c >= j + 3 && c < n) ? a * a : 0.0;
-    double x0 = (c == j + 2) ? a : 0.0;
-    sum2(sq, x0, 0);
+    if (wid < nwc) {
+      sq = warp_sum(sq);
+      if (lane == 0) s_part[buf][wid] = sq;
+    }
+    bar_named(1, T);
+    sq = 0.0;
+    for (int q = 0; q < nwc; ++q) sq += s_part[buf][q];
+    const double x0 = s_x0[buf];
     double u0n = 0.0, taun = 0.0, en = x0;
     if (more) eig_reflector(x0, sq, u0n, taun, en);
-    if (c == j + 1) V.d[j + 1] = a;
     if (t == 0) {
       V.e[j + 1] = en;
       if (more) {
@@ -192,51 +212,49 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
       }
     }
     if (c >= j + 2 && c < n) R1[c] = (c == j + 2 && more) ? u0n : a;
-    sync();
-    // (c)
-    const int r = j + 2 + t;
-    double pn = 0.0, urn = 0.0;
+    bar_named(1, T);
+    // (b)
+    const int r = j + 2 + rs;
+    double p = 0.0;
     if (r < n) {
       double* Rr = A + r * lda;
       const double ur = Uj[r], wr = W[r];
       double p0 = 0.0, p1 = 0.0;
-      int cc = j + 2;
-      for (; cc + 3 < n; cc += 4) {
-        double x[4], uj[4], wv[4], un[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          x[q] = Rr[cc + q];
-          uj[q] = Uj[cc + q];
-          wv[q] = W[cc + q];
-          un[q] = R1[cc + q];
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          x[q] = fma(-ur, wv[q], fma(-wr, uj[q], x[q]));
-          Rr[cc + q] = x[q];
-        }
-        p0 = fma(x[0], un[0], p0);
-        p1 = fma(x[1], un[1], p1);
-        p0 = fma(x[2], un[2], p0);
-        p1 = fma(x[3], un[3], p1);
+      int cc = j + 2 + seg;
+      for (; cc + 4 < n; cc += 8) {
+        const double x0v = Rr[cc], x1v = Rr[cc + 4];
+        const double u0v = Uj[cc], u1v = Uj[cc + 4];
+        const double w0v = W[cc], w1v = W[cc + 4];
+        const double n0v = R1[cc], n1v = R1[cc + 4];
+        const double y0 = fma(-ur, w0v, fma(-wr, u0v, x0v));
+        const double y1 = fma(-ur, w1v, fma(-wr, u1v, x1v));
+        Rr[cc] = y0;
+        Rr[cc + 4] = y1;
+        p0 = fma(y0, n0v, p0);
+        p1 = fma(y1, n1v, p1);
       }
-      for (; cc < n; ++cc) {
-        const double xv = fma(-ur, W[cc], fma(-wr, Uj[cc], Rr[cc]));
-        Rr[cc] = xv;
-        p0 = fma(xv, R1[cc], p0);
+      if (cc < n) {
+        const double y0 = fma(-ur, W[cc], fma(-wr, Uj[cc], Rr[cc]));
+        Rr[cc] = y0;
+        p0 = fma(y0, R1[cc], p0);
+        if (!more) V.d[n - 1] = y0;  // j = n-3: the single element of row n-1
       }
-      pn = taun * (p0 + p1);
-      urn = R1[r];
-      if (more) P[r] = pn;
-      if (!more) V.d[n - 1] = Rr[n - 1];  // r == n-1: the last diagonal
+      p = p0 + p1;
     }
     if (more) {
-      double kp = pn * urn, zero = 0.0;
-      sum2(kp, zero, 1);
-      K = 0.5 * taun * kp;
+      p += __shfl_xor_sync(~0u, p, 8);
+      p += __shfl_xor_sync(~0u, p, 16);
+      p *= taun;
+      double kp = 0.0;
+      if (r < n && seg == 0) {
+        P[r] = p;
+        kp = p * R1[r];
+      }
+      kp_partial(kp, buf);
     }
+    bar_named(1, T);
+    if (more) K = 0.5 * taun * kp_total(buf);
     tau = taun;
-    sync();
   }
 }
 
@@ -468,8 +486,7 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
     __syncthreads();
     return;
   }
-  const int nwa = (n - 1 + 31) / 32;
-  if (warp < nwa) eig_tridiag(A, lda, n, V, nwa);
+  if (warp < eig_tridiag_warps(n)) eig_tridiag(A, lda, n, V);
   __syncthreads();
   clk.mark(10);
 

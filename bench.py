@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=600, help="reference iterations timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--groups", type=int, default=0, help="CTAs per Hamiltonian column (0: the library's choice)")
     return ap.parse_args()
 
 
@@ -232,6 +233,7 @@ def b200_arm(args, rank, world, local_rank):
     import torch
 
     import mcdfci_b200 as mc
+    from mcdfci_b200.replicas import max_over_ranks, replica_rate
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -243,7 +245,7 @@ def b200_arm(args, rank, world, local_rank):
         path = write_workload(tmp, args.seed)
         fc = mc.Fcidump(path)
         solver = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
-                          z_threshold=args.z_threshold, threshold=0.0, device=local_rank)
+                          z_threshold=args.z_threshold, threshold=0.0, device=local_rank, groups=args.groups)
         solver.reset()
         solver.run_iterations(args.warmup)
         r0 = solver.report()
@@ -264,13 +266,8 @@ def b200_arm(args, rank, world, local_rank):
         entries = r1["emitted_total"] - r0["emitted_total"]
         updates = args.k * args.steps
         col_ms_avg = t["column_ms"] / args.steps
-        if dist:
-            tt = torch.tensor([total_s], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_max = float(tt.item())
-        else:
-            total_max = total_s
-        value = world * updates / total_max
+        total_max = max_over_ranks(total_s, dist, "cuda")
+        value = replica_rate(updates, total_s, world, dist, "cuda")
         solver.close()
 
         peak, peak_kind = hbm_peak()
@@ -286,9 +283,7 @@ def b200_arm(args, rank, world, local_rank):
         if not args.no_e2e:
             e2e = e2e_run(mc, fc, args, local_rank)
             if dist:
-                tt = torch.tensor([e2e["seconds"]], dtype=torch.float64, device="cuda")
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                e2e["value"] = world * args.k * e2e["iterations"] / float(tt.item())
+                e2e["value"] = replica_rate(args.k * e2e["iterations"], e2e["seconds"], world, dist, "cuda")
 
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_EXE):
@@ -334,7 +329,7 @@ def e2e_run(mc, fc, args, local_rank):
     t0 = time.perf_counter()
     s = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                  z_threshold=args.z_threshold, threshold=0.0, device=local_rank, num_iterations=iters,
-                 report_interval=interval)
+                 report_interval=interval, groups=args.groups)
     s.solve()
     energy = s.result_energy
     s.close()

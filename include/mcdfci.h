@@ -48,6 +48,7 @@ extern "C" {
 #define MCD_UPDATE_LS 2 /* accepted by the reference but not implemented here: MCD_ERR_UNSUPPORTED */
 
 typedef struct mcd_solver mcd_solver;   /* opaque: one solver bound to one GPU */
+typedef struct mcd_batch mcd_batch;     /* opaque: several solver instances advanced together on one GPU */
 typedef struct mcd_fcidump mcd_fcidump; /* opaque: a parsed FCIDUMP (host memory) */
 
 /* Integrals in spin-orbital form, as the reference's Fcidump holds them
@@ -106,6 +107,10 @@ typedef struct mcd_report {
 /* Called after every report_interval iterations; return nonzero to stop. */
 typedef int (*mcd_report_cb)(const mcd_report* report, void* user);
 
+/* Called for each instance of a batch after every report_interval
+ * iterations; return nonzero to stop the batch. */
+typedef int (*mcd_batch_report_cb)(int32_t instance, const mcd_report* report, void* user);
+
 /* ---- Input ------------------------------------------------------------- */
 
 /* Fcidump::Fcidump(path) (src/input.h:88-152). */
@@ -152,6 +157,30 @@ int mcd_result(const mcd_solver* s, double* energy);
 int mcd_stream(const mcd_solver* s, void** stream);
 /* Solver-side scalars: xx, scale, xz as (hi, lo) pairs; iteration count. */
 int mcd_scalars(mcd_solver* s, double xx[2], double scale[2], double xz[2], int64_t* iteration);
+
+/* ---- Batches ------------------------------------------------------------
+ *
+ * No counterpart in the reference, which solves several systems (the points
+ * of a binding curve) one after another with separate runs
+ * (experiments/4.4-binding-curve/dissociation.sh:2-9).  A batch holds up to 64
+ * instances, each an FCIDUMP of its own size with its own hash wavefunction
+ * of options->max_memory GB, all with the same options (k, m, z_threshold,
+ * num_iterations, report_interval; z_threshold_search is not supported).  One
+ * iteration advances every instance with two launches: one leader CTA per
+ * instance and the column CTAs of all instances in one grid; each instance
+ * computes exactly what it would alone. */
+int mcd_batch_create(const mcd_fcidump* const* fcidumps, int32_t n, const mcd_options* options, mcd_batch** out);
+void mcd_batch_destroy(mcd_batch* b);
+int mcd_batch_size(const mcd_batch* b, int32_t* n);
+/* Initial state of every instance, then num_iterations iterations with a
+ * report of each instance every report_interval (callback may be NULL). */
+int mcd_batch_solve(mcd_batch* b, mcd_batch_report_cb cb, void* user);
+int mcd_batch_reset(mcd_batch* b);
+int mcd_batch_run_iterations(mcd_batch* b, int64_t n);
+int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, double* column_ms, double* total_ms);
+int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r);
+/* Energies of the last batch solve, one per instance. */
+int mcd_batch_result(const mcd_batch* b, double* energies);
 
 /* Text of the last error on this thread. */
 const char* mcd_last_error(void);

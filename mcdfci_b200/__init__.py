@@ -41,6 +41,8 @@ EXPORTED_SYMBOLS = (
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
     "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_launch_info", "mcd_debug_leader_sections",
     "mcd_eig_update_static",
+    "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
+    "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
 )
 
 
@@ -88,6 +90,7 @@ class mcd_report(ctypes.Structure):
 
 
 REPORT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(mcd_report), ctypes.c_void_p)
+BATCH_REPORT_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int32, ctypes.POINTER(mcd_report), ctypes.c_void_p)
 
 _lib = None
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -131,6 +134,16 @@ def library() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_int32)]
     L.mcd_eig_update_static.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         ctypes.POINTER(ctypes.c_int32), vp]
+    L.mcd_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
+    L.mcd_batch_destroy.argtypes = [vp]
+    L.mcd_batch_destroy.restype = None
+    L.mcd_batch_size.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_batch_solve.argtypes = [vp, BATCH_REPORT_CB, vp]
+    L.mcd_batch_reset.argtypes = [vp]
+    L.mcd_batch_run_iterations.argtypes = [vp, ctypes.c_int64]
+    L.mcd_batch_run_iterations_timed.argtypes = [vp, ctypes.c_int64, _dp, _dp, _dp]
+    L.mcd_batch_get_report.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(mcd_report)]
+    L.mcd_batch_result.argtypes = [vp, _dp]
     L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
@@ -419,6 +432,76 @@ class CDFCI:
         _check(library().mcd_debug_picked(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
                                           dx.ctypes.data_as(_dp), cap, ctypes.byref(k)))
         return a[: k.value], b[: k.value], dx[: k.value]
+
+
+class CDFCIBatch:
+    """Several mCDFCI instances on one GPU, advanced together (mcd_batch_*).
+
+    ``CDFCIBatch([Fcidump(p) for p in paths], num_of_coordinate=16,
+    estimate=16, max_memory=1.0, num_iterations=20000, report_interval=1000)``
+    gives every FCIDUMP its own Hamiltonian tables and hash wavefunction;
+    ``solve()`` runs all of them and returns their energies.  The reference
+    has no equivalent: it solves a curve one point after another.
+    """
+
+    def __init__(self, sources, **options):
+        L = library()
+        self._fcidumps = [s if isinstance(s, Fcidump) else Fcidump(str(s)) for s in sources]
+        self._opts = make_options(**options)
+        arr = (ctypes.c_void_p * len(self._fcidumps))(*[f._h.value if isinstance(f._h, ctypes.c_void_p) else f._h
+                                                          for f in self._fcidumps])
+        h = ctypes.c_void_p()
+        _check(L.mcd_batch_create(arr, len(self._fcidumps), ctypes.byref(self._opts), ctypes.byref(h)))
+        self._h = h
+        self.reports: List[List[dict]] = [[] for _ in self._fcidumps]
+
+    def __len__(self) -> int:
+        return len(self._fcidumps)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().mcd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, callback: Optional[Callable[[int, dict], bool]] = None) -> List[float]:
+        self.reports = [[] for _ in self._fcidumps]
+
+        def cb(i, rep, _user):
+            d = rep.contents.as_dict()
+            self.reports[i].append(d)
+            return 1 if (callback is not None and callback(i, d)) else 0
+
+        c = BATCH_REPORT_CB(cb)
+        rc = library().mcd_batch_solve(self._h, c, None)
+        if rc not in (MCD_OK, MCD_STOPPED):
+            _check(rc)
+        return self.result_energies
+
+    @property
+    def result_energies(self) -> List[float]:
+        e = (ctypes.c_double * len(self))()
+        _check(library().mcd_batch_result(self._h, e))
+        return list(e)
+
+    def reset(self):
+        _check(library().mcd_batch_reset(self._h))
+
+    def run_iterations(self, n: int):
+        _check(library().mcd_batch_run_iterations(self._h, int(n)))
+
+    def run_iterations_timed(self, n: int) -> dict:
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(library().mcd_batch_run_iterations_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b),
+                                                        ctypes.byref(c)))
+        return {"leader_ms": a.value, "column_ms": b.value, "total_ms": c.value}
+
+    def report(self, i: int) -> dict:
+        r = mcd_report()
+        _check(library().mcd_batch_get_report(self._h, int(i), ctypes.byref(r)))
+        return r.as_dict()
 
 
 def debug_eig(hsub, x, z, xx, xz):

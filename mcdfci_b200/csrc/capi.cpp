@@ -13,11 +13,16 @@
 
 #include "../../include/mcdfci.h"
 #include "fcidump.h"
+#include "gpu_batch.h"
 #include "gpu_solver.h"
 #include "json.h"
 
 struct mcd_solver {
   std::unique_ptr<mcd::GpuSolver> impl;
+};
+
+struct mcd_batch {
+  std::unique_ptr<mcd::GpuBatch> impl;
 };
 
 struct mcd_fcidump {
@@ -244,6 +249,79 @@ int mcd_create_from_fcidump(const mcd_fcidump* f, const mcd_options* options, mc
 }
 
 void mcd_destroy(mcd_solver* s) { delete s; }
+
+// ---- Batches ----------------------------------------------------------------
+
+int mcd_batch_create(const mcd_fcidump* const* fcidumps, int32_t n, const mcd_options* options, mcd_batch** out) {
+  return guarded([&] {
+    if (!fcidumps || !options || !out) return fail(MCD_ERR_INVALID, "NULL argument.");
+    *out = nullptr;
+    if (n < 1) return fail(MCD_ERR_INVALID, "a batch needs at least one FCIDUMP.");
+    std::vector<const mcd::Fcidump*> f;
+    for (int32_t i = 0; i < n; ++i) {
+      if (!fcidumps[i]) return fail(MCD_ERR_INVALID, "NULL FCIDUMP in the batch.");
+      f.push_back(&fcidumps[i]->f);
+    }
+    auto b = std::make_unique<mcd_batch>();
+    b->impl = std::make_unique<mcd::GpuBatch>(f, to_options(options));
+    *out = b.release();
+    return MCD_OK;
+  });
+}
+
+void mcd_batch_destroy(mcd_batch* b) { delete b; }
+
+int mcd_batch_size(const mcd_batch* b, int32_t* n) {
+  if (!b || !n) return fail(MCD_ERR_INVALID, "NULL argument.");
+  *n = b->impl->size();
+  return MCD_OK;
+}
+
+int mcd_batch_solve(mcd_batch* b, mcd_batch_report_cb cb, void* user) {
+  return guarded([&] {
+    if (!b) return fail(MCD_ERR_INVALID, "batch is NULL.");
+    return b->impl->solve(cb, user);
+  });
+}
+
+int mcd_batch_reset(mcd_batch* b) {
+  return guarded([&] {
+    if (!b) return fail(MCD_ERR_INVALID, "batch is NULL.");
+    b->impl->reset();
+    return MCD_OK;
+  });
+}
+
+int mcd_batch_run_iterations(mcd_batch* b, int64_t n) {
+  return guarded([&] {
+    if (!b) return fail(MCD_ERR_INVALID, "batch is NULL.");
+    b->impl->run_iterations(n);
+    return MCD_OK;
+  });
+}
+
+int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, double* column_ms, double* total_ms) {
+  return guarded([&] {
+    if (!b || !leader_ms || !column_ms || !total_ms) return fail(MCD_ERR_INVALID, "NULL argument.");
+    b->impl->run_iterations_timed(n, leader_ms, column_ms, total_ms);
+    return MCD_OK;
+  });
+}
+
+int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r) {
+  return guarded([&] {
+    if (!b || !r) return fail(MCD_ERR_INVALID, "NULL argument.");
+    if (instance < 0 || instance >= b->impl->size()) return fail(MCD_ERR_INVALID, "instance out of range.");
+    *r = b->impl->report(instance);
+    return MCD_OK;
+  });
+}
+
+int mcd_batch_result(const mcd_batch* b, double* energies) {
+  if (!b || !energies) return fail(MCD_ERR_INVALID, "NULL argument.");
+  for (int i = 0; i < b->impl->size(); ++i) energies[i] = b->impl->result_energy(i);
+  return MCD_OK;
+}
 
 int mcd_solve(mcd_solver* s, mcd_report_cb cb, void* user) {
   return guarded([&] {

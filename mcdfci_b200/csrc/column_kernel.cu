@@ -243,12 +243,14 @@ __device__ __forceinline__ void toplist_merge_global(TopList<R>& L, const unsign
   bitonic_merge_desc<R>(L);
 }
 
+// One CTA's share of one column: CTA `blk` of the launch described by L
+// (column blk / groups, slice blk % groups).
 template <int R>
-__global__ void __launch_bounds__(kNT, 3) column_kernel(ColumnLaunch L) {
+__device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   constexpr int M = 32 * R;
   const int G = L.groups;
-  const int col = blockIdx.x / G;
-  const int g = blockIdx.x - col * G;
+  const int col = blk / G;
+  const int g = blk - col * G;
   IterState* S = L.st;
   const int kcur = S->k_cur;
   if (col >= kcur) return;
@@ -407,6 +409,26 @@ __global__ void __launch_bounds__(kNT, 3) column_kernel(ColumnLaunch L) {
   }
 }
 
+template <int R>
+__global__ void __launch_bounds__(kNT, 3) column_kernel(ColumnLaunch L) {
+  column_body<R>(L, blockIdx.x);
+}
+
+// Several instances in one grid: CTAs [cta_begin[i], cta_begin[i+1]) belong
+// to instance i and keep the layout of its own launch.
+template <int R>
+__global__ void __launch_bounds__(kNT, 3) column_kernel_batch(ColumnBatch B) {
+  int lo = 0, hi = B.n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.cta_begin[mid] <= static_cast<int>(blockIdx.x))
+      lo = mid;
+    else
+      hi = mid;
+  }
+  column_body<R>(B.L[lo], static_cast<int>(blockIdx.x) - B.cta_begin[lo]);
+}
+
 __global__ void __launch_bounds__(kNT) debug_column_kernel(HamDev h, Det d, double hd, uint64_t* ao,
                                                            uint64_t* bo, double* vo, int cap, int* nout) {
   __shared__ Prelude P;
@@ -455,6 +477,19 @@ cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s) {
   if (a.m <= 32) return launch_column_r<1>(a, s);
   if (a.m <= 64) return launch_column_r<2>(a, s);
   return launch_column_r<4>(a, s);
+}
+
+cudaError_t launch_column_batch(const ColumnBatch& b, cudaStream_t s) {
+  if (b.n < 1 || b.n > kMaxBatch) return cudaErrorInvalidValue;
+  const int ctas = b.cta_begin[b.n];
+  const int m = b.L[0].m;
+  if (m <= 32)
+    column_kernel_batch<1><<<ctas, kNT, 0, s>>>(b);
+  else if (m <= 64)
+    column_kernel_batch<2><<<ctas, kNT, 0, s>>>(b);
+  else
+    column_kernel_batch<4><<<ctas, kNT, 0, s>>>(b);
+  return cudaGetLastError();
 }
 
 cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,

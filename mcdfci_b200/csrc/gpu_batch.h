@@ -1,0 +1,57 @@
+// Several independent mCDFCI instances (for example the points of a
+// dissociation curve, each its own FCIDUMP) advanced together on one GPU: one
+// leader CTA per instance and the column CTAs of all instances in one grid,
+// two launches per iteration for the whole batch, recorded 64 iterations at a
+// time in a CUDA graph.  Each instance keeps its own Hamiltonian tables, hash
+// table and iteration state (a GpuSolver on the batch's stream), and its CTA
+// layout is that of its own single-instance launch.  No counterpart in the
+// reference, which solves a curve one point after another
+// (experiments/4.4-binding-curve/dissociation.sh:2-9).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "gpu_solver.h"
+
+namespace mcd {
+
+class GpuBatch {
+ public:
+  // opt applies to every instance (k, m, z_threshold, max_memory per
+  // instance, num_iterations, report_interval); z_threshold_search is not
+  // supported in a batch.
+  GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions& opt);
+  ~GpuBatch();
+  GpuBatch(const GpuBatch&) = delete;
+  GpuBatch& operator=(const GpuBatch&) = delete;
+
+  int size() const { return static_cast<int>(inst_.size()); }
+  void reset();
+  void run_iterations(long long n);
+  void run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms);
+  mcd_report report(int i);
+  // num_iterations iterations of every instance, a report of each every
+  // report_interval; cb(instance, report) returning nonzero stops the batch.
+  int solve(int (*cb)(int, const mcd_report*, void*), void* user);
+  double result_energy(int i) const { return energies_.at(static_cast<size_t>(i)); }
+  GpuSolver& instance(int i) { return *inst_.at(static_cast<size_t>(i)); }
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  void check(cudaError_t e, const char* what);
+  void launch_iteration();
+  void build_graph();
+
+  SolverOptions opt_;
+  std::vector<std::unique_ptr<GpuSolver>> inst_;
+  std::unique_ptr<LeaderBatch> lb_;
+  std::unique_ptr<ColumnBatch> cb_;
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  cudaGraphExec_t graph_ = nullptr;
+  long long graph_iters_ = 0;
+  std::vector<double> energies_;
+};
+
+}  // namespace mcd

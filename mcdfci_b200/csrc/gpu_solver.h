@@ -77,6 +77,12 @@ class GpuSolver {
   long long table_capacity() const { return static_cast<long long>(capacity_); }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }
+  // Launch descriptors and the column CTA count, for running this instance
+  // inside a batch (GpuBatch) on the same stream.
+  const LeaderLaunch& leader_launch() const { return ll_; }
+  const ColumnLaunch& column_launch() const { return cl_; }
+  int column_ctas() const { return cl_.k_grid * cl_.groups; }
+  int device() const { return device_; }
   int list_size() const { return list_; }
   int entries_per_column() const { return entries_; }
 

@@ -92,6 +92,24 @@ struct LeaderLaunch {
   int k_req;
 };
 
+// Several independent instances advanced by the same two launches per
+// iteration: one leader CTA per instance, and the column CTAs of all
+// instances in one grid (instance i owns CTAs [cta_begin[i], cta_begin[i+1])).
+// Passed by value as kernel parameters (well under the 32 KB limit), so that
+// every CTA reads its instance's descriptor from the constant bank.  All
+// instances of a batch share k and m.
+constexpr int kMaxBatch = 64;
+struct LeaderBatch {
+  int n;
+  LeaderLaunch L[kMaxBatch];
+};
+struct ColumnBatch {
+  int n;
+  int cta_begin[kMaxBatch + 1];
+  ColumnLaunch L[kMaxBatch];
+};
+static_assert(sizeof(LeaderBatch) <= 32000 && sizeof(ColumnBatch) <= 32000, "kernel parameters above 32 KB");
+
 // Phases of the leader kernel timed into LeaderLaunch::sect: 0 state load,
 // 1 finish + prefix, 2 candidate gather (slots, dedupe, scores), 3 top-k,
 // 4 full sort when the k-th score is tied, 5 picked determinants, 6 H_sub,
@@ -108,6 +126,8 @@ int column_list_size(int m);
 int column_groups(int entries, int k);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
+cudaError_t launch_leader_batch(const LeaderBatch& b, cudaStream_t s);
+cudaError_t launch_column_batch(const ColumnBatch& b, cudaStream_t s);
 cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStream_t s);
 // Applies the pending end of the last iteration (z reinsert of the picked
 // determinants, xz += dot), so that reported energies and table contents are

@@ -443,7 +443,7 @@ __device__ bool topk_fast(const unsigned* us, const double* sc, int n, int k, un
 }
 
 
-__global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
+__device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(16) IterState sS;
   __shared__ int s_off[kMaxK + 1];
@@ -731,6 +731,11 @@ __global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) {
 
 // Initial state (CDFCI::solve, src/solver.h:862-873): x = e_ref, z = H[:,ref]
 // through one column update with dx = 1, xx = scale = 1, xz = 0.
+__global__ void __launch_bounds__(kLT, 1) leader_kernel(LeaderLaunch L) { leader_body(L); }
+
+// One CTA per instance of a batch.
+__global__ void __launch_bounds__(kLT, 1) leader_kernel_batch(LeaderBatch B) { leader_body(B.L[blockIdx.x]); }
+
 __global__ void init_kernel(LeaderLaunch L, Det ref, double ref_diag) {
   IterState* S = L.st;
   bool inserted = false;
@@ -829,6 +834,20 @@ cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s) {
     configured = bytes;
   }
   leader_kernel<<<1, kLT, bytes, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leader_batch(const LeaderBatch& b, cudaStream_t s) {
+  if (b.n < 1 || b.n > kMaxBatch) return cudaErrorInvalidValue;
+  const size_t bytes = leader_smem_bytes(b.L[0].k_req, b.L[0].m);
+  static size_t configured = 0;
+  if (bytes > configured) {
+    cudaError_t e = cudaFuncSetAttribute(leader_kernel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    configured = bytes;
+  }
+  leader_kernel_batch<<<b.n, kLT, bytes, s>>>(b);
   return cudaGetLastError();
 }
 

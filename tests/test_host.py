@@ -100,3 +100,17 @@ def test_synth_deterministic_and_symmetric(tmp_path):
     _, h1c, e1, _ = synth.make_integrals("n16_5a5b", seed=0, t=1.0)
     _, hm, em, _ = synth.make_integrals("n16_5a5b", seed=0, t=0.5)
     assert np.allclose(hm, 0.5 * (h0 + h1c)) and np.allclose(em, 0.5 * (e0 + e1))
+
+
+def test_batch_rejects_before_gpu(fcidumps):
+    """Batch limits are checked on the host, before any device work."""
+    f = m.Fcidump(fcidumps["n7_5a5b"])
+    with pytest.raises(m.McdError) as e:
+        m.CDFCIBatch([], max_memory=0.001)
+    assert e.value.code == m.MCD_ERR_INVALID
+    with pytest.raises(m.McdError) as e:
+        m.CDFCIBatch([f] * 65, max_memory=0.001)
+    assert e.value.code == m.MCD_ERR_UNSUPPORTED
+    with pytest.raises(m.McdError) as e:
+        m.CDFCIBatch([f, f], max_memory=0.001, z_threshold_search=True, report_interval=1000)
+    assert e.value.code == m.MCD_ERR_UNSUPPORTED

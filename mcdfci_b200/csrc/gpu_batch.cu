@@ -1,11 +1,21 @@
 #include "gpu_batch.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <iomanip>
 #include <iostream>
 
 namespace mcd {
+
+// Concurrent groups of a batch: two let one group's leader CTAs (one SM each)
+// run under the other group's column grid.
+#ifndef MCD_BATCH_GROUPS
+#define MCD_BATCH_GROUPS 2
+#endif
+namespace {
+constexpr int kBatchGroups = MCD_BATCH_GROUPS;
+}  // namespace
 
 void GpuBatch::check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw McdError(MCD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -17,105 +27,143 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
   if (opt_.z_threshold_search)
     throw McdError(MCD_ERR_UNSUPPORTED, "z_threshold_search is not supported in a batch.");
   if (opt_.device >= 0) check(cudaSetDevice(opt_.device), "cudaSetDevice");
-  if (opt_.stream) {
-    stream_ = opt_.stream;
-  } else {
-    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-    own_stream_ = true;
-  }
+  const int ng = std::min(kBatchGroups, static_cast<int>(fcis.size()));
   try {
-    SolverOptions each = opt_;
-    each.stream = stream_;
-    each.verbose = false;
-    for (const Fcidump* f : fcis) inst_.push_back(std::make_unique<GpuSolver>(*f, each));
-    lb_ = std::make_unique<LeaderBatch>();
-    cb_ = std::make_unique<ColumnBatch>();
-    lb_->n = cb_->n = size();
-    cb_->cta_begin[0] = 0;
-    for (int i = 0; i < size(); ++i) {
-      lb_->L[i] = inst_[i]->leader_launch();
-      cb_->L[i] = inst_[i]->column_launch();
-      cb_->cta_begin[i + 1] = cb_->cta_begin[i] + inst_[i]->column_ctas();
+    if (opt_.stream) {
+      stream_ = opt_.stream;
+    } else {
+      check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+      own_stream_ = true;
+    }
+    groups_.resize(static_cast<size_t>(ng));
+    join_.assign(static_cast<size_t>(ng), nullptr);
+    for (int g = 0; g < ng; ++g) {
+      if (g == 0)
+        groups_[0].stream = stream_;
+      else
+        check(cudaStreamCreateWithFlags(&groups_[g].stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      check(cudaEventCreateWithFlags(&join_[g], cudaEventDisableTiming), "cudaEventCreate");
+      groups_[g].lb = std::make_unique<LeaderBatch>();
+      groups_[g].cb = std::make_unique<ColumnBatch>();
+      groups_[g].lb->n = groups_[g].cb->n = 0;
+      groups_[g].cb->cta_begin[0] = 0;
+    }
+    // Instance i goes to group i % ng, on that group's stream.
+    for (size_t i = 0; i < fcis.size(); ++i) {
+      Group& G = groups_[i % static_cast<size_t>(ng)];
+      SolverOptions each = opt_;
+      each.stream = G.stream;
+      each.verbose = false;
+      inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
+      const int j = G.lb->n;
+      G.lb->L[j] = inst_.back()->leader_launch();
+      G.cb->L[j] = inst_.back()->column_launch();
+      G.cb->cta_begin[j + 1] = G.cb->cta_begin[j] + inst_.back()->column_ctas();
+      G.lb->n = G.cb->n = j + 1;
     }
     energies_.assign(fcis.size(), 0.0);
   } catch (...) {
     inst_.clear();
-    if (own_stream_) cudaStreamDestroy(stream_);
+    for (size_t g = 0; g < groups_.size(); ++g)
+      if (g > 0 && groups_[g].stream) cudaStreamDestroy(groups_[g].stream);
+    for (auto e : join_)
+      if (e) cudaEventDestroy(e);
+    if (own_stream_ && stream_) cudaStreamDestroy(stream_);
     throw;
   }
 }
 
 GpuBatch::~GpuBatch() {
-  if (graph_) cudaGraphExecDestroy(graph_);
+  for (size_t g = 0; g < groups_.size(); ++g) {
+    if (groups_[g].graph) cudaGraphExecDestroy(groups_[g].graph);
+  }
   inst_.clear();
+  for (size_t g = 1; g < groups_.size(); ++g)
+    if (groups_[g].stream) cudaStreamDestroy(groups_[g].stream);
+  for (auto e : join_)
+    if (e) cudaEventDestroy(e);
   if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+// Make every group's stream wait for the others' enqueued work, so that a
+// later operation on any of them (a report, a reset) sees all of it.
+void GpuBatch::join_streams() {
+  for (size_t g = 0; g < groups_.size(); ++g) check(cudaEventRecord(join_[g], groups_[g].stream), "cudaEventRecord");
+  for (size_t g = 0; g < groups_.size(); ++g)
+    for (size_t h = 0; h < groups_.size(); ++h)
+      if (g != h) check(cudaStreamWaitEvent(groups_[g].stream, join_[h], 0), "cudaStreamWaitEvent");
 }
 
 void GpuBatch::reset() {
   for (auto& s : inst_) s->reset();
+  join_streams();
 }
 
-void GpuBatch::launch_iteration() {
-  check(launch_leader_batch(*lb_, stream_), "batched leader");
-  check(launch_column_batch(*cb_, stream_), "batched column");
+void GpuBatch::launch_iteration(Group& g) {
+  check(launch_leader_batch(*g.lb, g.stream), "batched leader");
+  check(launch_column_batch(*g.cb, g.stream), "batched column");
 }
 
-void GpuBatch::build_graph() {
-  launch_iteration();  // sets launch attributes outside capture
+void GpuBatch::build_graphs() {
   graph_iters_ = 64;
-  cudaGraph_t g = nullptr;
-  check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-  for (long long i = 0; i < graph_iters_; ++i) {
-    launch_leader_batch(*lb_, stream_);
-    launch_column_batch(*cb_, stream_);
+  for (Group& G : groups_) {
+    launch_iteration(G);  // sets launch attributes outside capture
+    cudaGraph_t g = nullptr;
+    check(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (long long i = 0; i < graph_iters_; ++i) {
+      launch_leader_batch(*G.lb, G.stream);
+      launch_column_batch(*G.cb, G.stream);
+    }
+    check(cudaStreamEndCapture(G.stream, &g), "end capture");
+    check(cudaGraphInstantiate(&G.graph, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
   }
-  check(cudaStreamEndCapture(stream_, &g), "end capture");
-  check(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
-  cudaGraphDestroy(g);
 }
 
 void GpuBatch::run_iterations(long long n) {
   if (n <= 0) return;
-  if (!graph_) {
-    build_graph();
+  if (!groups_[0].graph) {
+    build_graphs();
     --n;
   }
   while (n >= graph_iters_) {
-    check(cudaGraphLaunch(graph_, stream_), "graph launch");
+    for (Group& G : groups_) check(cudaGraphLaunch(G.graph, G.stream), "graph launch");
     n -= graph_iters_;
   }
-  for (; n > 0; --n) launch_iteration();
+  for (; n > 0; --n)
+    for (Group& G : groups_) launch_iteration(G);
+  join_streams();
 }
 
+// Device time of n iterations of the whole batch (CUDA events on group 0's
+// stream around work that every group joins).  With the groups overlapping,
+// the time is not split by kernel: leader_ms and column_ms stay 0.
 void GpuBatch::run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms) {
   *leader_ms = *column_ms = *total_ms = 0.0;
   if (n <= 0) return;
-  std::vector<cudaEvent_t> ev(static_cast<size_t>(2 * n + 1));
-  for (auto& e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
+  if (!groups_[0].graph) build_graphs();
+  cudaEvent_t a = nullptr, b = nullptr;
+  check(cudaEventCreate(&a), "cudaEventCreate");
+  check(cudaEventCreate(&b), "cudaEventCreate");
   try {
-    check(cudaEventRecord(ev[0], stream_), "cudaEventRecord");
-    for (long long i = 0; i < n; ++i) {
-      check(launch_leader_batch(*lb_, stream_), "batched leader");
-      check(cudaEventRecord(ev[2 * i + 1], stream_), "cudaEventRecord");
-      check(launch_column_batch(*cb_, stream_), "batched column");
-      check(cudaEventRecord(ev[2 * i + 2], stream_), "cudaEventRecord");
-    }
-    check(cudaEventSynchronize(ev[2 * n]), "cudaEventSynchronize");
-    for (long long i = 0; i < n; ++i) {
-      float a = 0.f, b = 0.f;
-      check(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]), "cudaEventElapsedTime");
-      check(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]), "cudaEventElapsedTime");
-      *leader_ms += a;
-      *column_ms += b;
-    }
+    join_streams();
+    check(cudaEventRecord(a, stream_), "cudaEventRecord");
+    join_streams();
+    for (long long i = 0; i < n; ++i)
+      for (Group& G : groups_) launch_iteration(G);
+    join_streams();
+    check(cudaEventRecord(b, stream_), "cudaEventRecord");
+    check(cudaEventSynchronize(b), "cudaEventSynchronize");
     float t = 0.f;
-    check(cudaEventElapsedTime(&t, ev[0], ev[2 * n]), "cudaEventElapsedTime");
+    check(cudaEventElapsedTime(&t, a, b), "cudaEventElapsedTime");
     *total_ms = t;
   } catch (...) {
-    for (auto& e : ev) cudaEventDestroy(e);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
     throw;
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
 }
 
 mcd_report GpuBatch::report(int i) { return inst_.at(static_cast<size_t>(i))->report(); }

@@ -1,8 +1,10 @@
 // Several independent mCDFCI instances (for example the points of a
-// dissociation curve, each its own FCIDUMP) advanced together on one GPU: one
-// leader CTA per instance and the column CTAs of all instances in one grid,
-// two launches per iteration for the whole batch, recorded 64 iterations at a
-// time in a CUDA graph.  Each instance keeps its own Hamiltonian tables, hash
+// dissociation curve, each its own FCIDUMP) advanced together on one GPU.
+// The instances are split into a few groups, each on its own stream: one
+// leader CTA per instance of the group and the column CTAs of the whole group
+// in one grid, two launches per iteration per group, recorded 64 iterations
+// at a time in a CUDA graph.  The groups run concurrently, so that one group's
+// single-SM leader CTAs overlap another group's column grid.  Each instance keeps its own Hamiltonian tables, hash
 // table and iteration state (a GpuSolver on the batch's stream), and its CTA
 // layout is that of its own single-instance launch.  No counterpart in the
 // reference, which solves a curve one point after another
@@ -40,16 +42,23 @@ class GpuBatch {
 
  private:
   void check(cudaError_t e, const char* what);
-  void launch_iteration();
-  void build_graph();
+
+  struct Group {
+    std::unique_ptr<LeaderBatch> lb;
+    std::unique_ptr<ColumnBatch> cb;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+  };
+  void join_streams();
+  void launch_iteration(Group& g);
+  void build_graphs();
 
   SolverOptions opt_;
   std::vector<std::unique_ptr<GpuSolver>> inst_;
-  std::unique_ptr<LeaderBatch> lb_;
-  std::unique_ptr<ColumnBatch> cb_;
-  cudaStream_t stream_ = nullptr;
+  std::vector<Group> groups_;
+  std::vector<cudaEvent_t> join_;  // one per group: the end of its last enqueued work
+  cudaStream_t stream_ = nullptr;  // group 0's stream; the others wait on it and it waits on them
   bool own_stream_ = false;
-  cudaGraphExec_t graph_ = nullptr;
   long long graph_iters_ = 0;
   std::vector<double> energies_;
 };

@@ -19,11 +19,20 @@ eigenproblem, apply x += dx and z += H_col * dx in the hash wavefunction.
   cpu_baseline the reference cdfci_omp, compiled from its sources, on a
                bounded sample of the same workload on this host's cores
 
+  batched      the 32-point dissociation curve (synthetic n16_5a5b points,
+               k = m = 16, 1 GB table each): coordinate updates/s of all 32
+               instances advanced together (mcd_batch_*) against one instance
+               on its own, from CUDA events
+
 Multi-GPU: the iteration does not shard (a sequential block Gauss-Southwell
 chain), so --gpus N runs N independent replicas with no collective on the
 data path ("weak" scaling).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --workload curve [--curve-iterations N]
+      time for the whole 32-point curve, batched against one point after
+      another, both through the public API, and the time until every point's
+      energy is within 1e-6 Ha of the energy it reaches after N iterations
 """
 import argparse
 import json
@@ -64,6 +73,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--groups", type=int, default=0, help="CTAs per Hamiltonian column (0: the library's choice)")
+    ap.add_argument("--workload", choices=["n24", "curve"], default="n24")
+    ap.add_argument("--curve-points", type=int, default=32)
+    ap.add_argument("--curve-iterations", type=int, default=20000)
+    ap.add_argument("--curve-report", type=int, default=1000)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-curve throughput object")
     return ap.parse_args()
 
 
@@ -153,6 +167,115 @@ def ncu_traffic():
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
     return float(m.group(1)) if m else None
+
+
+CURVE = "n16_5a5b"
+CURVE_K = 16
+CURVE_GB = 1.0
+
+
+def write_curve(d, points, seed):
+    """The dissociation-curve points: integrals interpolated between two
+    endpoints, the second with its off-diagonal couplings scaled x3."""
+    from mcdfci_b200 import synth
+
+    paths = []
+    for i in range(points):
+        t = i / (points - 1) if points > 1 else 0.0
+        p = os.path.join(d, f"{CURVE}_t{i:02d}.fcidump")
+        synth.write_fcidump(p, CURVE, seed=seed, t=t)
+        paths.append(p)
+    return paths
+
+
+def curve_throughput(mc, paths, local_rank, steps=500, warmup=500):
+    """Device-timed coordinate updates/s: the whole curve as one batch, and
+    one point on its own."""
+    opts = dict(num_of_coordinate=CURVE_K, estimate=CURVE_K, max_memory=CURVE_GB, z_threshold=0.0,
+                threshold=0.0, device=local_rank)
+    fc = [mc.Fcidump(p) for p in paths]
+    b = mc.CDFCIBatch(fc, **opts)
+    b.reset()
+    b.run_iterations(warmup)
+    tb = b.run_iterations_timed(steps)["total_ms"]
+    b.close()
+    s = mc.CDFCI(fc[0], **opts)
+    s.reset()
+    s.run_iterations(warmup)
+    ts = s.run_iterations_timed(steps)["total_ms"]
+    s.close()
+    batched = len(paths) * CURVE_K * steps / (tb / 1000.0)
+    plain = CURVE_K * steps / (ts / 1000.0)
+    return {"workload": f"{len(paths)} x {CURVE} curve points, k = m = {CURVE_K}, {CURVE_GB} GB table each",
+            "batched_updates_per_s": batched, "one_point_updates_per_s": plain,
+            "batched_ms_per_iteration": tb / steps, "one_point_ms_per_iteration": ts / steps,
+            "speedup_over_one_point_at_a_time": batched / plain,
+            "timing": f"CUDA events, {steps} iterations after {warmup}"}
+
+
+def curve_arm(args, local_rank):
+    """The curve solved both ways through the public API (create + solve +
+    reports + result, wall clock), and the time until every point is within
+    1e-6 Ha of the energy the batch reaches after N iterations."""
+    import mcdfci_b200 as mc
+
+    n_it, rep = args.curve_iterations, args.curve_report
+    opts = dict(num_of_coordinate=CURVE_K, estimate=CURVE_K, max_memory=CURVE_GB, z_threshold=0.0,
+                threshold=0.0, device=local_rank, num_iterations=n_it, report_interval=rep)
+    tmp = tempfile.mkdtemp(prefix="mcd_curve_")
+    try:
+        paths = write_curve(tmp, args.curve_points, args.seed)
+        fc = [mc.Fcidump(p) for p in paths]
+        t0 = time.perf_counter()
+        b = mc.CDFCIBatch(fc, **opts)
+        t_ready = time.perf_counter()
+        eb = b.solve()
+        t_batch = time.perf_counter() - t0
+        hist_b = [[(r["time_s"], r["energy"]) for r in reps] for reps in b.reports]
+        b.close()
+        plain_times, hist_p, ep = [], [], []
+        for f in fc:
+            t1 = time.perf_counter()
+            s = mc.CDFCI(f, **opts)
+            ts_ready = time.perf_counter() - t1
+            ep.append(s.solve())
+            plain_times.append(time.perf_counter() - t1)
+            hist_p.append([(ts_ready + r["time_s"], r["energy"]) for r in s.reports])
+            s.close()
+        tol = 1e-6
+        # Away from convergence the two runs of a point follow different
+        # trajectories (the pick order depends on the order of concurrent
+        # atomic updates), so each point's target is the energy level both
+        # of its runs reach: max(final batched, final plain) + 1e-6 Ha.
+        level = [max(a, c) + tol for a, c in zip(eb, ep)]
+
+        def first_at(hist, lvl):
+            for t, e in hist:
+                if e <= lvl:
+                    return t
+            return None
+
+        tb = [first_at(h, level[i]) for i, h in enumerate(hist_b)]
+        tp = [first_at(h, level[i]) for i, h in enumerate(hist_p)]
+        t_b = (t_ready - t0) + max(tb) if all(x is not None for x in tb) else None
+        t_p = sum(tp) if all(x is not None for x in tp) else None
+        out = {
+            "metric": "time to E within 1e-6 Ha, batched vs plain", "unit": "s", "higher_is_better": False,
+            "value": t_b, "plain_value": t_p, "speedup": (t_p / t_b) if (t_b and t_p) else None,
+            "target": (f"per point, the energy both its batched and its one-at-a-time run reach in {n_it} "
+                       "iterations, within 1e-6 Ha; batched: set-up + the time the last point gets there; "
+                       "plain: sum over points of set-up + time to get there"),
+            "curve_wall_s": {"batched": t_batch, "plain_sum": sum(plain_times)},
+            "max_abs_energy_difference_batched_vs_plain": max(abs(a - c) for a, c in zip(eb, ep)),
+            "energies": {"first": eb[0], "last": eb[-1]},
+            "config": {"workload": f"{len(paths)} x {CURVE} points (t = 0..1), k = m = {CURVE_K}, "
+                                   f"{CURVE_GB} GB table each", "iterations": n_it, "report_interval": rep},
+            "n_gpus": 1, "dtype": "f64", "data": "synthetic (mcdfci_b200.synth)",
+        }
+        print(json.dumps(out))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
 
 
 def write_workload(d, seed):
@@ -285,6 +408,11 @@ def b200_arm(args, rank, world, local_rank):
             if dist:
                 e2e["value"] = replica_rate(args.k * e2e["iterations"], e2e["seconds"], world, dist, "cuda")
 
+        batched = None
+        if not args.no_batched:
+            ctmp = tempfile.mkdtemp(prefix="mcd_curve_", dir=tmp)
+            batched = curve_throughput(mc, write_curve(ctmp, args.curve_points, args.seed), local_rank)
+
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_EXE):
             threads = os.cpu_count() or 1
@@ -309,6 +437,7 @@ def b200_arm(args, rank, world, local_rank):
                 "gpu_launches": 2 * args.steps,
                 "roofline": roofline,
                 "cpu_baseline": cpu,
+                "batched": batched,
                 "clocks": clocks,
                 "energy": r1["energy"],
                 "z_size": r1["z_size"],
@@ -353,6 +482,13 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload == "curve":
+        if world > 1 and rank != 0:
+            return 0
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        return curve_arm(args, local_rank)
     if world > 1:
         import datetime
 

@@ -59,6 +59,9 @@ struct EigVecs {
 
 // Householder scalars for x = (x0, rest) with |rest|^2 = s: u = x + sign(x0)
 // mu e_1 maps x to e e_1 with e = -sign(x0) mu; u'u = 2 mu |u0|, tau = 2/u'u.
+// Both roots come from the reciprocal square root (about 1 ulp each), with no
+// division on the chain: mu = q rsqrt(q), tau = rsqrt(mu |u0|)^2, which keeps
+// H_j orthogonal to a few ulp.
 __device__ __forceinline__ void eig_reflector(double x0, double s, double& u0, double& tau, double& e) {
   if (s == 0.0) {  // nothing to annihilate: H = I
     u0 = 0.0;
@@ -66,10 +69,12 @@ __device__ __forceinline__ void eig_reflector(double x0, double s, double& u0, d
     e = x0;
     return;
   }
-  const double mu = sqrt(fma(x0, x0, s));
+  const double q = fma(x0, x0, s);
+  const double mu = q * rsqrt(q);
   const double sg = x0 < 0.0 ? -1.0 : 1.0;
   u0 = fma(sg, mu, x0);
-  tau = 1.0 / (mu * fabs(u0));
+  const double r = rsqrt(mu * fabs(u0));
+  tau = r * r;
   e = -sg * mu;
 }
 
@@ -115,9 +120,20 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
     v = warp_sum(v);
     if (lane == 0) s_kp[buf][wid] = v;
   };
-  auto kp_total = [&](int buf) {
+  auto part_total = [&](int buf) {
+    double v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = q < nwc ? s_part[buf][q] : 0.0;
+    return (v[0] + v[1]) + (v[2] + v[3]);
+  };
+  // The per-warp partials, loaded together and summed in a fixed order.
+  auto kp_total = [&](int buf) {  // 4 nwc partials, four at a time
     double k = 0.0;
-    for (int q = 0; q < T / 32; ++q) k += s_kp[buf][q];
+    for (int g = 0; g < nwc; ++g) {
+      const double v0 = s_kp[buf][4 * g], v1 = s_kp[buf][4 * g + 1];
+      const double v2 = s_kp[buf][4 * g + 2], v3 = s_kp[buf][4 * g + 3];
+      k += (v0 + v1) + (v2 + v3);
+    }
     return k;
   };
 
@@ -136,8 +152,7 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
       if (lane == 0) s_part[0][wid] = sq;
     }
     bar_named(1, T);
-    sq = 0.0;
-    for (int q = 0; q < nwc; ++q) sq += s_part[0][q];
+    sq = part_total(0);
     double u0, e0;
     eig_reflector(s_x0[0], sq, u0, tau, e0);
     if (t == 0) {
@@ -199,8 +214,7 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
       if (lane == 0) s_part[buf][wid] = sq;
     }
     bar_named(1, T);
-    sq = 0.0;
-    for (int q = 0; q < nwc; ++q) sq += s_part[buf][q];
+    sq = part_total(buf);
     const double x0 = s_x0[buf];
     double u0n = 0.0, taun = 0.0, en = x0;
     if (more) eig_reflector(x0, sq, u0n, taun, en);

@@ -182,6 +182,20 @@ int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r);
 /* Energies of the last batch solve, one per instance. */
 int mcd_batch_result(const mcd_batch* b, double* energies);
 
+/* ---- Energy gradient ------------------------------------------------------
+ *
+ * No counterpart in the reference.  The energy is variational, so its
+ * derivative with respect to the integrals is the reduced density matrices of
+ * the wavefunction: dE/dh_PQ = rdm1[P][Q] and dE/d(PR|QS) = rdm2[P][Q][R][S]/2
+ * for independent entries of the dense spatial integral arrays.  mcd_rdm
+ * computes them from the current wavefunction on the GPU (one pass over the
+ * determinants with nonzero coefficients, recomputing their single and double
+ * excitations): rdm1[P*n+Q] = sum_s <a+_{Ps} a_{Qs}>, rdm2[((P*n+Q)*n+R)*n+S] =
+ * sum_{s,t} <a+_{Ps} a+_{Qt} a_{St} a_{Rs}>, normalised, n spatial orbitals,
+ * so that E = sum h_PQ rdm1[P][Q] + 1/2 sum (PR|QS) rdm2[P][Q][R][S] + E_core.
+ * RHF FCIDUMPs only (MCD_ERR_UNSUPPORTED for UHF). */
+int mcd_rdm(mcd_solver* s, double* rdm1, double* rdm2);
+
 /* Text of the last error on this thread. */
 const char* mcd_last_error(void);
 
@@ -235,6 +249,9 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
  * back-transformation, Rayleigh quotient, eig finish), summed over launches
  * since the previous call, which resets them.  No counterpart in the reference. */
 int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n);
+/* The determinants with nonzero x and their x (the coefficients are scale * x),
+ * sorted by slot; up to cap of them, *n_out receives the count. */
+int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, int64_t cap, int64_t* n_out);
 /* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);
 

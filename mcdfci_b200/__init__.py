@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
+    "mcd_rdm", "mcd_debug_wavefunction",
 )
 
 
@@ -134,6 +135,8 @@ def library() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_int32)]
     L.mcd_eig_update_static.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         ctypes.POINTER(ctypes.c_int32), vp]
+    L.mcd_rdm.argtypes = [vp, _dp, _dp]
+    L.mcd_debug_wavefunction.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     L.mcd_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
     L.mcd_batch_destroy.argtypes = [vp]
     L.mcd_batch_destroy.restype = None
@@ -312,6 +315,8 @@ class CDFCI:
             _check(L.mcd_create_from_fcidump(self._fcidump._h, ctypes.byref(self._opts), ctypes.byref(h)))
         self._h = h
         self.reports: List[dict] = []
+        # spatial orbitals (the problem counts spin-orbitals)
+        self.norb = (source.norb if isinstance(source, mcd_problem) else self._fcidump.norb) // 2
 
     def close(self):
         if getattr(self, "_h", None):
@@ -360,6 +365,32 @@ class CDFCI:
         r = mcd_report()
         _check(library().mcd_get_report(self._h, ctypes.byref(r)))
         return r.as_dict()
+
+    def rdm(self):
+        """Spin-summed spatial 1- and 2-RDM of the current wavefunction
+        (mcd_rdm): arrays [n, n] and [n, n, n, n]."""
+        import numpy as np
+
+        n = self.norb
+        g1 = np.zeros(n * n)
+        g2 = np.zeros(n ** 4)
+        _check(library().mcd_rdm(self._h, g1.ctypes.data_as(_dp), g2.ctypes.data_as(_dp)))
+        return g1.reshape(n, n), g2.reshape(n, n, n, n)
+
+    def wavefunction(self):
+        """(alpha, beta, x) of the determinants with nonzero x."""
+        import numpy as np
+
+        cnt = ctypes.c_int64()
+        _check(library().mcd_debug_wavefunction(self._h, None, None, None, 0, ctypes.byref(cnt)))
+        n = cnt.value + 16
+        a = np.zeros(n, dtype=np.uint64)
+        b = np.zeros(n, dtype=np.uint64)
+        x = np.zeros(n)
+        _check(library().mcd_debug_wavefunction(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
+                                                x.ctypes.data_as(_dp), n, ctypes.byref(cnt)))
+        k = min(cnt.value, n)
+        return a[:k], b[:k], x[:k]
 
     @property
     def stream(self) -> int:

@@ -3,6 +3,7 @@
 // thread for mcd_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <iomanip>
@@ -524,6 +525,34 @@ int mcd_eig_update_static(int32_t k, const double* hsub, const double* x, const 
     new_scale[1] = out[1].lo;
     if (branch) *branch = br;
     if (err) return fail(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
+    return MCD_OK;
+  });
+}
+
+int mcd_rdm(mcd_solver* s, double* rdm1, double* rdm2) {
+  return guarded([&] {
+    if (!s || !rdm1 || !rdm2) return fail(MCD_ERR_INVALID, "NULL argument.");
+    std::vector<double> g1, g2;
+    s->impl->rdm(g1, g2);
+    std::copy(g1.begin(), g1.end(), rdm1);
+    std::copy(g2.begin(), g2.end(), rdm2);
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, int64_t cap, int64_t* n_out) {
+  return guarded([&] {
+    if (!s || !n_out) return fail(MCD_ERR_INVALID, "NULL argument.");
+    std::vector<mcd::Det> d;
+    std::vector<double> v;
+    s->impl->wavefunction(d, v);
+    *n_out = static_cast<int64_t>(d.size());
+    const int64_t m = std::min<int64_t>(cap, static_cast<int64_t>(d.size()));
+    for (int64_t i = 0; i < m; ++i) {
+      if (alpha) alpha[i] = d[static_cast<size_t>(i)].a;
+      if (beta) beta[i] = d[static_cast<size_t>(i)].b;
+      if (x) x[i] = v[static_cast<size_t>(i)];
+    }
     return MCD_OK;
   });
 }

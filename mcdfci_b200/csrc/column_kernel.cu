@@ -455,6 +455,200 @@ cudaError_t launch_column_r(const ColumnLaunch& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Reduced density matrices of the wavefunction in the table (the adjoint of
+// the energy with respect to the integrals).  One CTA per determinant D with
+// x_D != 0: the diagonal terms over D's occupied pairs, then every single and
+// double excitation D' of D (all of them: the RDM is a property of the
+// wavefunction, so no integral screening) with x_D' looked up in the table.
+// The operator phases are those of the column generation, i.e. of
+// <D'|a+_r a_p|D> and <D'|a+_r a+_s a_q a_p|D> in the interleaved order.
+// Accumulated unnormalised, in spin blocks (see RdmLaunch).
+
+__global__ void rdm_list_kernel(const Slot* slots, size_t n, unsigned* list, unsigned long long* count,
+                                unsigned long long cap) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Slot sl = slots[i];
+    if (sl.a == kEmptyKey && sl.b == kEmptyKey) continue;
+    if (sl.x == 0.0) continue;
+    const unsigned long long j = atomicAdd(count, 1ull);
+    if (j < cap) list[j] = static_cast<unsigned>(i);
+  }
+}
+
+// Canonical index of a same-spin pair block element: (p, q) and (r, s) put in
+// increasing order; returns the sign of the reordering.
+__device__ __forceinline__ double pair_canon(int& p, int& q) {
+  if (p < q) return 1.0;
+  const int t = p;
+  p = q;
+  q = t;
+  return -1.0;
+}
+
+__device__ __forceinline__ size_t idx4(int n, int p, int q, int r, int s) {
+  return ((static_cast<size_t>(p) * n + q) * n + r) * n + s;
+}
+
+__global__ void __launch_bounds__(kNT) rdm_kernel(RdmLaunch R) {
+  __shared__ Prelude P;
+  const int n = R.ham.norb;
+  const int warp = threadIdx.x >> 5;
+  for (long long li = blockIdx.x; li < R.nlist; li += gridDim.x) {
+    const Slot* sd = R.tab.slots + R.list[li];
+    const Det D{sd->a, sd->b};
+    const double xd = sd->x;
+    __syncthreads();  // P of the previous determinant is no longer read
+    if (warp == 0) build_prelude(P, D, n);
+    __syncthreads();
+    // Diagonal: gamma_pp, Gamma_pqpq over occupied pairs.
+    {
+      const double w = xd * xd;
+      const int na = P.na, nb = P.nb;
+      for (int t = threadIdx.x; t < na + nb; t += blockDim.x) {
+        if (t < na)
+          atomicAdd(R.g1a + static_cast<size_t>(P.occA[t]) * n + P.occA[t], w);
+        else
+          atomicAdd(R.g1b + static_cast<size_t>(P.occB[t - na]) * n + P.occB[t - na], w);
+      }
+      for (int t = threadIdx.x; t < na * na; t += blockDim.x) {
+        const int i = t / na, j = t - i * na;
+        if (i < j) {
+          const int p = P.occA[i], q = P.occA[j];
+          atomicAdd(R.g2aa + idx4(n, p, q, p, q), w);
+        }
+      }
+      for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+        const int i = t / nb, j = t - i * nb;
+        if (i < j) {
+          const int p = P.occB[i], q = P.occB[j];
+          atomicAdd(R.g2bb + idx4(n, p, q, p, q), w);
+        }
+      }
+      for (int t = threadIdx.x; t < na * nb; t += blockDim.x) {
+        const int i = t / nb, j = t - i * nb;
+        const int p = P.occA[i], q = P.occB[j];
+        atomicAdd(R.g2ab + idx4(n, p, q, p, q), w);
+      }
+    }
+    // Excitations.
+    for (int e = 1 + threadIdx.x; e < P.total; e += blockDim.x) {
+      const uint64_t a = P.a, b = P.b;
+      int kind, p = 0, q = 0, r = 0, s = 0;
+      uint64_t a2, b2;
+      bool neg;
+      if (e < P.off2) {
+        const int t = e - 1;
+        const int i = t / P.va;
+        p = P.occA[i];
+        r = P.virA[t - i * P.va];
+        kind = 1;
+        neg = sign_alpha(a, b, p, r);
+        a2 = a ^ (1ull << p) ^ (1ull << r);
+        b2 = b;
+      } else if (e < P.off3) {
+        const int t = e - P.off2;
+        const int i = t / P.vb;
+        p = P.occB[i];
+        r = P.virB[t - i * P.vb];
+        kind = 2;
+        neg = sign_beta(a, b, p, r);
+        a2 = a;
+        b2 = b ^ (1ull << p) ^ (1ull << r);
+      } else if (e < P.off4) {
+        const int t = e - P.off3;
+        const int op = t / P.ca_vir, vp = t - op * P.ca_vir;
+        int i, j, ri, sj;
+        pair_decode(op, i, j);
+        pair_decode(vp, ri, sj);
+        p = P.occA[i];
+        q = P.occA[j];
+        r = P.virA[ri];
+        s = P.virA[sj];
+        kind = 3;
+        neg = sign_aa(a, b, p, q, r, s);
+        a2 = a ^ (1ull << p) ^ (1ull << q) ^ (1ull << r) ^ (1ull << s);
+        b2 = b;
+      } else if (e < P.off5) {
+        const int t = e - P.off4;
+        const int op = t / P.cb_vir, vp = t - op * P.cb_vir;
+        int i, j, ri, sj;
+        pair_decode(op, i, j);
+        pair_decode(vp, ri, sj);
+        p = P.occB[i];
+        q = P.occB[j];
+        r = P.virB[ri];
+        s = P.virB[sj];
+        kind = 4;
+        neg = sign_bb(a, b, p, q, r, s);
+        a2 = a;
+        b2 = b ^ (1ull << p) ^ (1ull << q) ^ (1ull << r) ^ (1ull << s);
+      } else {
+        int t = e - P.off5;
+        const int sbi = t % P.vb;
+        t /= P.vb;
+        const int rai = t % P.va;
+        t /= P.va;
+        const int pbi = t % P.nb;
+        const int pai = t / P.nb;
+        p = P.occA[pai];  // alpha: p -> r
+        r = P.virA[rai];
+        q = P.occB[pbi];  // beta: q -> s
+        s = P.virB[sbi];
+        kind = 5;
+        neg = sign_ab(a, b, p, r, q, s);
+        a2 = a ^ (1ull << p) ^ (1ull << r);
+        b2 = b ^ (1ull << q) ^ (1ull << s);
+      }
+      const long long slot = table_find(R.tab, a2, b2);
+      if (slot < 0) continue;
+      const double x2 = R.tab.slots[slot].x;
+      if (x2 == 0.0) continue;
+      const double w = neg ? -(xd * x2) : xd * x2;
+      switch (kind) {
+        case 1:  // <a+_r a_p> and the spectators k: <a+_r a+_k a_k a_p>
+          atomicAdd(R.g1a + static_cast<size_t>(r) * n + p, w);
+          for (int x = 0; x < P.na; ++x) {
+            const int k = P.occA[x];
+            if (k == p) continue;
+            int c1 = r, c2 = k, d1 = p, d2 = k;
+            const double sg = pair_canon(c1, c2) * pair_canon(d1, d2);
+            atomicAdd(R.g2aa + idx4(n, c1, c2, d1, d2), sg * w);
+          }
+          for (int x = 0; x < P.nb; ++x) {
+            const int k = P.occB[x];
+            atomicAdd(R.g2ab + idx4(n, r, k, p, k), w);
+          }
+          break;
+        case 2:
+          atomicAdd(R.g1b + static_cast<size_t>(r) * n + p, w);
+          for (int x = 0; x < P.nb; ++x) {
+            const int k = P.occB[x];
+            if (k == p) continue;
+            int c1 = r, c2 = k, d1 = p, d2 = k;
+            const double sg = pair_canon(c1, c2) * pair_canon(d1, d2);
+            atomicAdd(R.g2bb + idx4(n, c1, c2, d1, d2), sg * w);
+          }
+          for (int x = 0; x < P.na; ++x) {
+            const int k = P.occA[x];
+            atomicAdd(R.g2ab + idx4(n, k, r, k, p), w);
+          }
+          break;
+        case 3:  // <a+_r a+_s a_q a_p>, p < q, r < s
+          atomicAdd(R.g2aa + idx4(n, r, s, p, q), w);
+          break;
+        case 4:
+          atomicAdd(R.g2bb + idx4(n, r, s, p, q), w);
+          break;
+        default:  // <a+_r(alpha) a+_s(beta) a_q(beta) a_p(alpha)>
+          atomicAdd(R.g2ab + idx4(n, r, s, p, q), w);
+          break;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 int column_entries(int norb, int na, int nb) {
@@ -489,6 +683,19 @@ cudaError_t launch_column_batch(const ColumnBatch& b, cudaStream_t s) {
     column_kernel_batch<2><<<ctas, kNT, 0, s>>>(b);
   else
     column_kernel_batch<4><<<ctas, kNT, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rdm_list(const TableDev& t, size_t capacity, unsigned* list, unsigned long long* count,
+                            unsigned long long cap, cudaStream_t s) {
+  rdm_list_kernel<<<148 * 8, 256, 0, s>>>(t.slots, capacity, list, count, cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s) {
+  if (r.nlist <= 0) return cudaSuccess;
+  const long long blocks = r.nlist < 148LL * 16 ? r.nlist : 148LL * 16;
+  rdm_kernel<<<static_cast<unsigned>(blocks), kNT, 0, s>>>(r);
   return cudaGetLastError();
 }
 

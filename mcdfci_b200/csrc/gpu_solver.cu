@@ -111,6 +111,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     throw McdError(MCD_ERR_UNSUPPORTED, "estimate must be in 1.." + std::to_string(kMaxM) + ".");
   if (opt_.groups < 0) throw McdError(MCD_ERR_INVALID, "groups must be >= 0.");
   zt_ = opt_.z_threshold;
+  uhf_ = fci.uhf;
   if (opt_.z_threshold_search && zt_ < 1e-10) zt_ = 1e-10;
 
   try {
@@ -402,6 +403,113 @@ mcd_report GpuSolver::report() {
   check(cudaMemcpy(&r.occupied, d_occ_, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "occupancy read");
   r.last_k = h_state_.k_cur;
   return r;
+}
+
+void GpuSolver::wavefunction(std::vector<Det>& dets, std::vector<double>& x) {
+  read_state();
+  const unsigned long long cap = h_state_.x_size + 64;
+  unsigned* d_list = device_alloc<unsigned>(cap, "x list");
+  unsigned long long* d_count = nullptr;
+  try {
+    d_count = device_alloc<unsigned long long>(1, "x count");
+    check(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), stream_), "memset");
+    check(launch_rdm_list(td_, capacity_, d_list, d_count, cap, stream_), "x list");
+    unsigned long long cnt = 0;
+    check(cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, stream_), "count read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    if (cnt > cap) throw McdError(MCD_ERR_CUDA, "more nonzero coefficients than x_size counted");
+    std::vector<unsigned> list(cnt);
+    if (cnt) check(cudaMemcpy(list.data(), d_list, cnt * sizeof(unsigned), cudaMemcpyDeviceToHost), "list read");
+    std::sort(list.begin(), list.end());
+    dets.resize(cnt);
+    x.resize(cnt);
+    for (size_t i = 0; i < cnt; ++i) {
+      Slot sl;
+      check(cudaMemcpy(&sl, d_slots_ + list[i], sizeof(Slot), cudaMemcpyDeviceToHost), "slot read");
+      dets[i] = Det{sl.a, sl.b};
+      x[i] = sl.x;
+    }
+  } catch (...) {
+    cudaFree(d_list);
+    if (d_count) cudaFree(d_count);
+    throw;
+  }
+  cudaFree(d_list);
+  cudaFree(d_count);
+}
+
+void GpuSolver::rdm(std::vector<double>& rdm1, std::vector<double>& rdm2) {
+  if (uhf_) throw McdError(MCD_ERR_UNSUPPORTED, "RDMs are implemented for RHF FCIDUMPs.");
+  read_state();
+  const int n = ham_.norb;
+  const size_t n2 = static_cast<size_t>(n) * n, n4 = n2 * n2;
+  const unsigned long long cap = h_state_.x_size + 64;
+  std::vector<void*> owned;
+  auto alloc = [&](size_t bytes, const char* what) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      for (void* q : owned) cudaFree(q);
+      throw McdError(MCD_ERR_CUDA, std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    }
+    owned.push_back(p);
+    return p;
+  };
+  try {
+    auto* d_list = static_cast<unsigned*>(alloc(cap * sizeof(unsigned), "rdm list"));
+    auto* d_count = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long), "rdm count"));
+    auto* d_g = static_cast<double*>(alloc((2 * n2 + 3 * n4) * sizeof(double), "rdm"));
+    check(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), stream_), "memset");
+    check(cudaMemsetAsync(d_g, 0, (2 * n2 + 3 * n4) * sizeof(double), stream_), "memset");
+    check(launch_rdm_list(td_, capacity_, d_list, d_count, cap, stream_), "rdm list");
+    unsigned long long cnt = 0;
+    check(cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, stream_), "count read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    if (cnt > cap) throw McdError(MCD_ERR_CUDA, "more nonzero coefficients than x_size counted");
+    RdmLaunch r{};
+    r.ham = hd_;
+    r.tab = td_;
+    r.list = d_list;
+    r.nlist = static_cast<long long>(cnt);
+    r.g1a = d_g;
+    r.g1b = d_g + n2;
+    r.g2aa = d_g + 2 * n2;
+    r.g2bb = r.g2aa + n4;
+    r.g2ab = r.g2bb + n4;
+    check(launch_rdm(r, stream_), "rdm");
+    std::vector<double> g(2 * n2 + 3 * n4);
+    check(cudaMemcpyAsync(g.data(), d_g, g.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "rdm read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    for (void* q : owned) cudaFree(q);
+    owned.clear();
+    const double norm = 1.0 / dd_to_d(h_state_.xx);
+    const double* g1a = g.data();
+    const double* g1b = g1a + n2;
+    const double* aa = g1b + n2;
+    const double* bb = aa + n4;
+    const double* ab = bb + n4;
+    rdm1.assign(n2, 0.0);
+    rdm2.assign(n4, 0.0);
+    for (size_t i = 0; i < n2; ++i) rdm1[i] = (g1a[i] + g1b[i]) * norm;
+    auto I = [n](int p, int q, int r, int s) { return ((static_cast<size_t>(p) * n + q) * n + r) * n + s; };
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q < n; ++q)
+        for (int r = 0; r < n; ++r)
+          for (int s2 = 0; s2 < n; ++s2) {
+            // Same-spin blocks from their canonical p < q, r < s elements.
+            double same = 0.0;
+            if (p != q && r != s2) {
+              const int cp = p < q ? p : q, cq = p < q ? q : p, cr = r < s2 ? r : s2, cs = r < s2 ? s2 : r;
+              const double sg = ((p < q) ? 1.0 : -1.0) * ((r < s2) ? 1.0 : -1.0);
+              same = sg * (aa[I(cp, cq, cr, cs)] + bb[I(cp, cq, cr, cs)]);
+            }
+            // Opposite spins: (alpha, beta) + (beta, alpha) = ab[p][q][r][s] + ab[q][p][s][r].
+            rdm2[I(p, q, r, s2)] = (same + ab[I(p, q, r, s2)] + ab[I(q, p, s2, r)]) * norm;
+          }
+  } catch (...) {
+    for (void* q : owned) cudaFree(q);
+    throw;
+  }
 }
 
 void GpuSolver::scalars(dd* xx, dd* scale, dd* xz, long long* iter) {

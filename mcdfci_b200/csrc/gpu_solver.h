@@ -69,6 +69,13 @@ class GpuSolver {
   std::vector<double> hsub(const std::vector<Det>& dets);
   void table_sums(dd* xx, dd* xz, unsigned long long* occupied);
   std::vector<std::pair<Det, double>> picked();
+  // Spin-summed spatial 1- and 2-RDM of the current wavefunction, normalised
+  // (rdm1[P*n+Q] = sum_s <a+_{Ps} a_{Qs}>, rdm2[((P*n+Q)*n+R)*n+S] =
+  // sum_{s,t} <a+_{Ps} a+_{Qt} a_{St} a_{Rs}>, n spatial orbitals), so that
+  // E = sum h_PQ rdm1 + 1/2 sum (PR|QS) rdm2 + E_core.
+  void rdm(std::vector<double>& rdm1, std::vector<double>& rdm2);
+  // The determinants with x != 0 and their x (scaled: coefficients are scale * x).
+  void wavefunction(std::vector<Det>& dets, std::vector<double>& x);
   // Leader-kernel phase timers (SM cycles summed over launches since the last call).
   std::vector<unsigned long long> leader_sections();
 
@@ -98,6 +105,7 @@ class GpuSolver {
   Det ref_{0, 0};
   double ref_diag_ = 0.0;
   int na_ = 0, nb_ = 0, entries_ = 0, groups_ = 1, list_ = 32, n_words_ = 1;
+  bool uhf_ = false;
   size_t capacity_ = 0;             // hash slots (power of two)
   unsigned long long max_size_ = 0; // reference max_wavefunction_size
   double zt_ = 0.0;

@@ -110,6 +110,20 @@ struct ColumnBatch {
 };
 static_assert(sizeof(LeaderBatch) <= 32000 && sizeof(ColumnBatch) <= 32000, "kernel parameters above 32 KB");
 
+// Reduced density matrices of the wavefunction in the table, unnormalised
+// (divide by sum x^2), in spin blocks over spatial orbitals (n = ham.norb):
+//   g1a[r*n+p]          = sum <a+_{r alpha} a_{p alpha}>           (g1b: beta)
+//   g2aa[((p*n+q)*n+r)*n+s], p < q, r < s only
+//                       = sum <a+_p a+_q a_s a_r> (all alpha)      (g2bb: beta)
+//   g2ab[((p*n+q)*n+r)*n+s] = sum <a+_{p alpha} a+_{q beta} a_{s beta} a_{r alpha}>
+struct RdmLaunch {
+  HamDev ham;
+  TableDev tab;
+  const unsigned* list;  // slots of the determinants with x != 0
+  long long nlist;
+  double *g1a, *g1b, *g2aa, *g2bb, *g2ab;
+};
+
 // Phases of the leader kernel timed into LeaderLaunch::sect: 0 state load,
 // 1 finish + prefix, 2 candidate gather (slots, dedupe, scores), 3 top-k,
 // 4 full sort when the k-th score is tied, 5 picked determinants, 6 H_sub,
@@ -137,6 +151,11 @@ cudaError_t launch_finish(const LeaderLaunch& a, cudaStream_t s);
 cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s);
 cudaError_t launch_table_sums(const Slot* slots, size_t n, dd* partial, unsigned long long* count, int nblocks,
                               cudaStream_t s);
+
+// Slots with x != 0 into list (up to cap; *count receives the total).
+cudaError_t launch_rdm_list(const TableDev& t, size_t capacity, unsigned* list, unsigned long long* count,
+                            unsigned long long cap, cudaStream_t s);
+cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s);
 
 // Debug / parity entry points (synchronous).
 // Column of one determinant: writes up to `cap` (a, b, value) entries.

@@ -134,3 +134,19 @@ def test_gradient_matches_finite_differences(fcidumps, tmp_path):
         em = _solve(out)[1]
         fd = (ep - em) / (2 * h)
         assert abs(fd - float(v0.grad[j])) < 1e-6, (lines[ids[j]], fd, float(v0.grad[j]))
+
+
+def test_rdm_energy_identity_n12(synth_fcidumps):
+    """The gradient workload (12 orbitals, 6 + 6 electrons, 853,776
+    determinants): after 3000 iterations the RDMs of the current vector give
+    the solver's energy (with z_threshold = 0 both are its Rayleigh quotient)."""
+    path = synth_fcidumps["n12_6a6b"]
+    s = m.CDFCI(m.Fcidump(path), num_of_coordinate=32, estimate=32, max_memory=1.0, threshold=0.0,
+                z_threshold=0.0)
+    s.reset()
+    s.run_iterations(3000)
+    e = s.report()["energy"]
+    g1, g2 = s.rdm()
+    n, ne, ms2, h, eri, ecore = ordm.read_fcidump(path)
+    assert abs(ordm.energy(h, eri, ecore, g1, g2) - e) < 1e-8
+    assert abs(np.trace(g1) - ne) < 1e-10

@@ -83,6 +83,11 @@ typedef struct mcd_options {
   int32_t verbose;             /* 1: print the reference's report table to stdout */
   void* stream;                /* cudaStream_t to run on; NULL = a stream owned by the solver */
   int32_t device;              /* CUDA device ordinal; -1 = the current device */
+  /* 1: compaction under max_memory (no counterpart in the reference): when the
+   * table passes 60% of its occupancy limit at a report, z_threshold doubles
+   * and the entries with x = 0 and |z scale| <= z_threshold are removed, until
+   * it is below 40%, instead of failing with MCD_ERR_OVERFLOW.  0 by default. */
+  int32_t compaction;
 } mcd_options;
 
 /* One line of the reference's report table (src/solver.h:761-798). */
@@ -236,6 +241,9 @@ int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* 
 int mcd_eig_update_static(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                           const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch,
                           void* stream);
+/* One compaction now (see mcd_options.compaction) with the given z_threshold
+ * (>= the current one); *occupied receives the slots in use after it. */
+int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied);
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
-    "mcd_rdm", "mcd_debug_wavefunction",
+    "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact",
 )
 
 
@@ -72,7 +72,7 @@ class mcd_options(ctypes.Structure):
         ("ref_det_occ", ctypes.POINTER(ctypes.c_int32)), ("n_ref_det_occ", ctypes.c_int32),
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
-        ("stream", ctypes.c_void_p), ("device", ctypes.c_int32),
+        ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
     ]
 
 
@@ -136,6 +136,7 @@ def library() -> ctypes.CDLL:
     L.mcd_eig_update_static.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         ctypes.POINTER(ctypes.c_int32), vp]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
+    L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
     L.mcd_debug_wavefunction.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     L.mcd_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
     L.mcd_batch_destroy.argtypes = [vp]
@@ -282,6 +283,8 @@ def make_options(**kw) -> mcd_options:
             o.stream = ctypes.c_void_p(int(v) if v else 0)
         elif k == "z_threshold_search":
             o.z_threshold_search = int(bool(v))
+        elif k == "compaction":
+            o.compaction = int(bool(v))
         else:
             setattr(o, k, v)
     if occ:
@@ -376,6 +379,12 @@ class CDFCI:
         g2 = np.zeros(n ** 4)
         _check(library().mcd_rdm(self._h, g1.ctypes.data_as(_dp), g2.ctypes.data_as(_dp)))
         return g1.reshape(n, n), g2.reshape(n, n, n, n)
+
+    def compact(self, z_threshold: float) -> int:
+        """One compaction with the given z_threshold; returns the occupied slots."""
+        occ = ctypes.c_uint64()
+        _check(library().mcd_debug_compact(self._h, float(z_threshold), ctypes.byref(occ)))
+        return occ.value
 
     def wavefunction(self):
         """(alpha, beta, x) of the determinants with nonzero x."""

@@ -70,6 +70,7 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.coordinate_pick = o->coordinate_pick;
   s.coordinate_update = o->coordinate_update;
   s.groups = o->groups;
+  s.compaction = o->compaction != 0;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -152,6 +153,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   o->max_memory = cd.at("max_memory").as_number("max_memory");
   o->threshold = option.at("hamiltonian").at("threshold").as_number("hamiltonian:threshold");
   if (cd.has("groups")) o->groups = static_cast<int32_t>(cd.at("groups").as_number("groups"));
+  if (cd.has("compaction")) o->compaction = cd.at("compaction").as_bool("compaction") ? 1 : 0;
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -186,6 +188,7 @@ void mcd_options_default(mcd_options* o) {
   o->coordinate_pick = MCD_PICK_GCD_GRAD;
   o->coordinate_update = MCD_UPDATE_EIG;
   o->groups = 0;
+  o->compaction = 0;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;
@@ -553,6 +556,15 @@ int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, doubl
       if (beta) beta[i] = d[static_cast<size_t>(i)].b;
       if (x) x[i] = v[static_cast<size_t>(i)];
     }
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    const unsigned long long occ = s->impl->compact(z_threshold);
+    if (occupied) *occupied = occ;
     return MCD_OK;
   });
 }

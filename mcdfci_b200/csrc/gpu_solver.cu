@@ -3,6 +3,7 @@
 #include "device_common.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -52,6 +53,105 @@ __global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsi
     }
     partial[2 * blockIdx.x] = t1;
     partial[2 * blockIdx.x + 1] = t2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Compaction: the slots that survive (x != 0, or |z| above a limit) are
+// copied in slot order into a buffer (per-block counts, then per-block
+// in-order writes at prefix-sum offsets, so that the survivor list depends
+// only on the table's contents), the table is cleared and they are inserted
+// again.  The current candidate lists are saved before and re-found after.
+
+__device__ __forceinline__ bool compact_keeps(const Slot& s, double zlim) {
+  if (s.a == kEmptyKey && s.b == kEmptyKey) return false;
+  return s.x != 0.0 || fabs(s.z) > zlim;
+}
+
+__global__ void compact_count_kernel(const Slot* slots, size_t n, size_t chunk, double zlim,
+                                     unsigned long long* counts) {
+  __shared__ unsigned long long ws[32];
+  const size_t beg = blockIdx.x * chunk, end = beg + chunk < n ? beg + chunk : n;
+  unsigned long long c = 0;
+  for (size_t i = beg + threadIdx.x; i < end; i += blockDim.x) c += compact_keeps(slots[i], zlim) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(~0u, c, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += ws[w];
+    counts[blockIdx.x] = t;
+  }
+}
+
+__global__ void compact_write_kernel(const Slot* slots, size_t n, size_t chunk, double zlim,
+                                     const unsigned long long* offsets, Slot* out) {
+  __shared__ unsigned ws[33];
+  const size_t beg = blockIdx.x * chunk, end = beg + chunk < n ? beg + chunk : n;
+  unsigned long long pos = offsets[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (size_t base = beg; base < end; base += blockDim.x) {
+    const size_t i = base + threadIdx.x;
+    Slot sl{};
+    const bool keep = i < end && compact_keeps(sl = slots[i], zlim);
+    const unsigned b = __ballot_sync(~0u, keep);
+    if (lane == 0) ws[warp] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned run = 0;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+        const unsigned c = ws[w];
+        ws[w] = run;
+        run += c;
+      }
+      ws[32] = run;
+    }
+    __syncthreads();
+    if (keep) out[pos + ws[warp] + __popc(b & lanemask_lt())] = sl;
+    pos += ws[32];
+    __syncthreads();
+  }
+}
+
+__global__ void compact_reinsert_kernel(TableDev t, const Slot* src, size_t cnt) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < cnt;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Slot s = src[i];
+    bool inserted;
+    const long long j = table_upsert(t, s.a, s.b, inserted);
+    if (j >= 0) {
+      t.slots[j].x = s.x;
+      t.slots[j].z = s.z;
+    }
+  }
+}
+
+// Candidate lists: (col < k_cur, i < cand_n[col]).  save: the slots'
+// contents; restore: find or insert each saved determinant, its new slot.
+__global__ void compact_cand_save_kernel(const Slot* slots, const IterState* st, const unsigned* cand_slot, int m,
+                                         Slot* saved) {
+  const int col = blockIdx.x;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    Slot e{kEmptyKey, kEmptyKey, 0.0, 0.0};
+    if (col < st->k_cur && i < st->cand_n[col]) e = slots[cand_slot[col * m + i]];
+    saved[col * m + i] = e;
+  }
+}
+
+__global__ void compact_cand_restore_kernel(TableDev t, const IterState* st, const Slot* saved, unsigned* cand_slot,
+                                            int m) {
+  const int col = blockIdx.x;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    if (!(col < st->k_cur && i < st->cand_n[col])) continue;
+    const Slot s = saved[col * m + i];
+    bool inserted;
+    const long long j = table_upsert(t, s.a, s.b, inserted);
+    if (j < 0) continue;  // table error word already set
+    if (inserted) {
+      t.slots[j].x = s.x;
+      t.slots[j].z = s.z;
+    }
+    cand_slot[col * m + i] = static_cast<unsigned>(j);
   }
 }
 
@@ -512,6 +612,72 @@ void GpuSolver::rdm(std::vector<double>& rdm1, std::vector<double>& rdm2) {
   }
 }
 
+unsigned long long GpuSolver::compact(double z_threshold) {
+  read_state();  // applies the pending end of the iteration; no work in flight
+  if (!(z_threshold >= zt_)) throw McdError(MCD_ERR_INVALID, "compaction needs z_threshold >= the current one.");
+  const double sc = std::fabs(dd_to_d(h_state_.scale));
+  // |dz scale| > zt is the insertion rule; |z scale| <= zt is dropped here.
+  const double zlim = z_threshold / std::max(sc, 1e-300);
+  const int nb = 148 * 8;
+  const size_t chunk = (capacity_ + nb - 1) / nb;
+  const int m = opt_.m;
+  std::vector<void*> owned;
+  auto alloc = [&](size_t bytes, const char* what) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess)
+      throw McdError(MCD_ERR_CUDA, std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    owned.push_back(p);
+    return p;
+  };
+  unsigned long long occ = 0;
+  try {
+    auto* d_counts = static_cast<unsigned long long*>(alloc(nb * sizeof(unsigned long long), "compaction counts"));
+    compact_count_kernel<<<nb, 256, 0, stream_>>>(d_slots_, capacity_, chunk, zlim, d_counts);
+    check(cudaGetLastError(), "compaction count");
+    std::vector<unsigned long long> counts(nb), offs(nb);
+    check(cudaMemcpyAsync(counts.data(), d_counts, nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+          "counts read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    unsigned long long total = 0;
+    for (int b = 0; b < nb; ++b) {
+      offs[b] = total;
+      total += counts[b];
+    }
+    check(cudaMemcpyAsync(d_counts, offs.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_),
+          "offsets");
+    auto* d_out = static_cast<Slot*>(alloc(std::max<unsigned long long>(total, 1) * sizeof(Slot), "compaction buffer"));
+    auto* d_saved = static_cast<Slot*>(alloc(static_cast<size_t>(kMaxK) * m * sizeof(Slot), "candidates"));
+    compact_cand_save_kernel<<<kMaxK, 128, 0, stream_>>>(d_slots_, d_state_, d_cand_slot_, m, d_saved);
+    check(cudaGetLastError(), "candidates save");
+    compact_write_kernel<<<nb, 256, 0, stream_>>>(d_slots_, capacity_, chunk, zlim, d_counts, d_out);
+    check(cudaGetLastError(), "compaction write");
+    check(launch_table_fill(d_slots_, capacity_, stream_), "table clear");
+    check(cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_), "memset");
+    compact_reinsert_kernel<<<148 * 8, 256, 0, stream_>>>(td_, d_out, total);
+    check(cudaGetLastError(), "reinsert");
+    compact_cand_restore_kernel<<<kMaxK, 128, 0, stream_>>>(td_, d_state_, d_saved, d_cand_slot_, m);
+    check(cudaGetLastError(), "candidates restore");
+    check(cudaMemcpyAsync(&occ, d_occ_, sizeof(occ), cudaMemcpyDeviceToHost, stream_), "occupancy read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    for (void* q : owned) cudaFree(q);
+    owned.clear();
+  } catch (...) {
+    for (void* q : owned) cudaFree(q);
+    throw;
+  }
+  zt_ = z_threshold;
+  h_state_.zt = zt_;
+  h_state_.z_size = occ;
+  check(cudaMemcpyAsync(reinterpret_cast<char*>(d_state_) + offsetof(IterState, zt), &h_state_.zt, sizeof(double),
+                        cudaMemcpyHostToDevice, stream_), "zt upload");
+  check(cudaMemcpyAsync(reinterpret_cast<char*>(d_state_) + offsetof(IterState, z_size), &h_state_.z_size,
+                        sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_), "z_size upload");
+  check(cudaStreamSynchronize(stream_), "synchronize");
+  read_state();
+  return occ;
+}
+
 void GpuSolver::scalars(dd* xx, dd* scale, dd* xz, long long* iter) {
   read_state();
   *xx = h_state_.xx;
@@ -583,6 +749,18 @@ int GpuSolver::solve(mcd_report_cb cb, void* user) {
           restart = true;
           break;
         }
+      }
+      // Compaction under max_memory: before the table fills, double
+      // z_threshold and drop the entries with x = 0 and |z scale| below it.
+      if (opt_.compaction && static_cast<double>(r.occupied) > 0.6 * static_cast<double>(h_state_.occupancy_limit)) {
+        unsigned long long occ = r.occupied;
+        for (int round = 0; round < 30 && static_cast<double>(occ) > 0.4 * static_cast<double>(h_state_.occupancy_limit);
+             ++round)
+          occ = compact(std::max(2.0 * zt_, 1e-10));
+        if (v)
+          std::cout << "compaction: z_threshold " << std::scientific << std::setprecision(2) << zt_ << ", |z|_0 "
+                    << occ << std::endl;
+        r.z_size = occ;
       }
       last_z = r.z_size;
       if (static_cast<double>(r.z_size) > 0.79 * static_cast<double>(max_size_))

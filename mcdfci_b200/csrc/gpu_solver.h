@@ -28,6 +28,7 @@ struct SolverOptions {
   int coordinate_pick = MCD_PICK_GCD_GRAD;
   int coordinate_update = MCD_UPDATE_EIG;
   int groups = 0;
+  bool compaction = false;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -74,6 +75,9 @@ class GpuSolver {
   // sum_{s,t} <a+_{Ps} a+_{Qt} a_{St} a_{Rs}>, n spatial orbitals), so that
   // E = sum h_PQ rdm1 + 1/2 sum (PR|QS) rdm2 + E_core.
   void rdm(std::vector<double>& rdm1, std::vector<double>& rdm2);
+  // Raise z_threshold to `z_threshold` and remove the entries with x = 0 and
+  // |z scale| <= z_threshold, rebuilding the table; returns the occupied slots.
+  unsigned long long compact(double z_threshold);
   // The determinants with x != 0 and their x (scaled: coefficients are scale * x).
   void wavefunction(std::vector<Det>& dets, std::vector<double>& x);
   // Leader-kernel phase timers (SM cycles summed over launches since the last call).

@@ -201,6 +201,18 @@ int mcd_batch_result(const mcd_batch* b, double* energies);
  * RHF FCIDUMPs only (MCD_ERR_UNSUPPORTED for UHF). */
 int mcd_rdm(mcd_solver* s, double* rdm1, double* rdm2);
 
+/* ---- Checkpoint / restart -------------------------------------------------
+ *
+ * No counterpart in the reference.  mcd_checkpoint_save writes the
+ * wavefunction (every occupied slot: determinant, x, z) and the iteration
+ * state (scalars in double-double, counters, candidate lists) to a binary
+ * file; mcd_checkpoint_load, on a solver created for the same FCIDUMP with the
+ * same num_of_coordinate and estimate, replaces its state with the file's, so
+ * that mcd_run_iterations continues the saved solve.  The table may differ in
+ * size (max_memory) if it holds the saved entries (else MCD_ERR_OVERFLOW). */
+int mcd_checkpoint_save(mcd_solver* s, const char* path);
+int mcd_checkpoint_load(mcd_solver* s, const char* path);
+
 /* Text of the last error on this thread. */
 const char* mcd_last_error(void);
 

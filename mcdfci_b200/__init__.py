@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
-    "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact",
+    "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
 )
 
 
@@ -137,6 +137,8 @@ def library() -> ctypes.CDLL:
                                         ctypes.POINTER(ctypes.c_int32), vp]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
     L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
+    L.mcd_checkpoint_save.argtypes = [vp, ctypes.c_char_p]
+    L.mcd_checkpoint_load.argtypes = [vp, ctypes.c_char_p]
     L.mcd_debug_wavefunction.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     L.mcd_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(mcd_options), ctypes.POINTER(vp)]
     L.mcd_batch_destroy.argtypes = [vp]
@@ -379,6 +381,14 @@ class CDFCI:
         g2 = np.zeros(n ** 4)
         _check(library().mcd_rdm(self._h, g1.ctypes.data_as(_dp), g2.ctypes.data_as(_dp)))
         return g1.reshape(n, n), g2.reshape(n, n, n, n)
+
+    def save(self, path: str):
+        """Checkpoint of the wavefunction and the iteration state."""
+        _check(library().mcd_checkpoint_save(self._h, str(path).encode()))
+
+    def load(self, path: str):
+        """Continue from a checkpoint of the same problem, k and m."""
+        _check(library().mcd_checkpoint_load(self._h, str(path).encode()))
 
     def compact(self, z_threshold: float) -> int:
         """One compaction with the given z_threshold; returns the occupied slots."""

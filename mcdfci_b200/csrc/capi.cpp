@@ -560,6 +560,22 @@ int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, doubl
   });
 }
 
+int mcd_checkpoint_save(mcd_solver* s, const char* path) {
+  return guarded([&] {
+    if (!s || !path) return fail(MCD_ERR_INVALID, "NULL argument.");
+    s->impl->checkpoint_save(path);
+    return MCD_OK;
+  });
+}
+
+int mcd_checkpoint_load(mcd_solver* s, const char* path) {
+  return guarded([&] {
+    if (!s || !path) return fail(MCD_ERR_INVALID, "NULL argument.");
+    s->impl->checkpoint_load(path);
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");

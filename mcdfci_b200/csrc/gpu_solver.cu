@@ -678,6 +678,149 @@ unsigned long long GpuSolver::compact(double z_threshold) {
   return occ;
 }
 
+// ---------------------------------------------------------------------------
+// Checkpoint: header, iteration state, the occupied slots in slot order and
+// the candidate lists by determinant; loading rebuilds the table by insertion.
+
+namespace {
+constexpr char kCkptMagic[8] = {'M', 'C', 'D', 'F', 'C', 'I', 'K', '1'};
+struct CkptHeader {
+  char magic[8];
+  int32_t nso, nelec, k, m;
+  double ecore;
+  uint64_t state_bytes, nslots, ncand;
+};
+}  // namespace
+
+void GpuSolver::gather_slots(double zlim, std::vector<Slot>& out) {
+  const int nb = 148 * 8;
+  const size_t chunk = (capacity_ + nb - 1) / nb;
+  unsigned long long* d_counts = device_alloc<unsigned long long>(nb, "gather counts");
+  Slot* d_out = nullptr;
+  try {
+    compact_count_kernel<<<nb, 256, 0, stream_>>>(d_slots_, capacity_, chunk, zlim, d_counts);
+    check(cudaGetLastError(), "gather count");
+    std::vector<unsigned long long> counts(nb), offs(nb);
+    check(cudaMemcpyAsync(counts.data(), d_counts, nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+          "counts read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+    unsigned long long total = 0;
+    for (int b = 0; b < nb; ++b) {
+      offs[b] = total;
+      total += counts[b];
+    }
+    check(cudaMemcpyAsync(d_counts, offs.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_),
+          "offsets");
+    d_out = device_alloc<Slot>(std::max<unsigned long long>(total, 1), "gather buffer");
+    compact_write_kernel<<<nb, 256, 0, stream_>>>(d_slots_, capacity_, chunk, zlim, d_counts, d_out);
+    check(cudaGetLastError(), "gather write");
+    out.resize(total);
+    if (total)
+      check(cudaMemcpyAsync(out.data(), d_out, total * sizeof(Slot), cudaMemcpyDeviceToHost, stream_), "slots read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+  } catch (...) {
+    cudaFree(d_counts);
+    if (d_out) cudaFree(d_out);
+    throw;
+  }
+  cudaFree(d_counts);
+  cudaFree(d_out);
+}
+
+void GpuSolver::checkpoint_save(const std::string& path) {
+  read_state();
+  std::vector<Slot> slots;
+  gather_slots(-1.0, slots);
+  const int m = opt_.m;
+  std::vector<Slot> cand(static_cast<size_t>(kMaxK) * m);
+  Slot* d_saved = device_alloc<Slot>(cand.size(), "candidates");
+  try {
+    compact_cand_save_kernel<<<kMaxK, 128, 0, stream_>>>(d_slots_, d_state_, d_cand_slot_, m, d_saved);
+    check(cudaGetLastError(), "candidates save");
+    check(cudaMemcpyAsync(cand.data(), d_saved, cand.size() * sizeof(Slot), cudaMemcpyDeviceToHost, stream_),
+          "candidates read");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+  } catch (...) {
+    cudaFree(d_saved);
+    throw;
+  }
+  cudaFree(d_saved);
+  CkptHeader h{};
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.nso = ham_.nso;
+  h.nelec = na_ + nb_;
+  h.k = opt_.k;
+  h.m = m;
+  h.ecore = ham_.ecore;
+  h.state_bytes = sizeof(IterState);
+  h.nslots = slots.size();
+  h.ncand = cand.size();
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) throw McdError(MCD_ERR_INVALID, "cannot write the checkpoint file " + path);
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(&h_state_, sizeof(IterState), 1, f) == 1 &&
+            (slots.empty() || std::fwrite(slots.data(), sizeof(Slot), slots.size(), f) == slots.size()) &&
+            std::fwrite(cand.data(), sizeof(Slot), cand.size(), f) == cand.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) throw McdError(MCD_ERR_INVALID, "writing the checkpoint file " + path + " failed");
+}
+
+void GpuSolver::checkpoint_load(const std::string& path) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw McdError(MCD_ERR_INVALID, "cannot read the checkpoint file " + path);
+  CkptHeader h{};
+  IterState st{};
+  std::vector<Slot> slots, cand;
+  bool ok = std::fread(&h, sizeof(h), 1, f) == 1;
+  if (ok && std::memcmp(h.magic, kCkptMagic, 8) != 0) ok = false;
+  if (ok && (h.nso != ham_.nso || h.nelec != na_ + nb_ || h.k != opt_.k || h.m != opt_.m || h.ecore != ham_.ecore ||
+             h.state_bytes != sizeof(IterState) || h.ncand != static_cast<uint64_t>(kMaxK) * opt_.m)) {
+    std::fclose(f);
+    throw McdError(MCD_ERR_INVALID, "the checkpoint " + path + " belongs to another problem or other options");
+  }
+  if (ok) ok = std::fread(&st, sizeof(st), 1, f) == 1;
+  if (ok) {
+    slots.resize(h.nslots);
+    cand.resize(h.ncand);
+    ok = (slots.empty() || std::fread(slots.data(), sizeof(Slot), slots.size(), f) == slots.size()) &&
+         std::fread(cand.data(), sizeof(Slot), cand.size(), f) == cand.size();
+  }
+  std::fclose(f);
+  if (!ok) throw McdError(MCD_ERR_INVALID, "the checkpoint file " + path + " is not readable");
+  const unsigned long long limit = static_cast<unsigned long long>(0.79 * static_cast<double>(max_size_));
+  if (slots.size() > limit)
+    throw McdError(MCD_ERR_OVERFLOW, "The hash table is full. Please increase max_memory or z_threshold.");
+  check(cudaStreamSynchronize(stream_), "synchronize");
+  Slot* d_in = device_alloc<Slot>(std::max<size_t>(slots.size(), 1), "checkpoint slots");
+  Slot* d_saved = nullptr;
+  try {
+    d_saved = device_alloc<Slot>(cand.size(), "checkpoint candidates");
+    if (!slots.empty())
+      check(cudaMemcpyAsync(d_in, slots.data(), slots.size() * sizeof(Slot), cudaMemcpyHostToDevice, stream_),
+            "slots upload");
+    check(cudaMemcpyAsync(d_saved, cand.data(), cand.size() * sizeof(Slot), cudaMemcpyHostToDevice, stream_),
+          "candidates upload");
+    st.occupancy_limit = limit;  // this table's, not the saved one's
+    st.pending = 0;
+    check(cudaMemcpyAsync(d_state_, &st, sizeof(IterState), cudaMemcpyHostToDevice, stream_), "state upload");
+    check(cudaMemsetAsync(d_err_, 0, sizeof(unsigned), stream_), "memset");
+    check(launch_table_fill(d_slots_, capacity_, stream_), "table clear");
+    check(cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_), "memset");
+    compact_reinsert_kernel<<<148 * 8, 256, 0, stream_>>>(td_, d_in, slots.size());
+    check(cudaGetLastError(), "reinsert");
+    compact_cand_restore_kernel<<<kMaxK, 128, 0, stream_>>>(td_, d_state_, d_saved, d_cand_slot_, opt_.m);
+    check(cudaGetLastError(), "candidates restore");
+    check(cudaStreamSynchronize(stream_), "synchronize");
+  } catch (...) {
+    cudaFree(d_in);
+    if (d_saved) cudaFree(d_saved);
+    throw;
+  }
+  cudaFree(d_in);
+  cudaFree(d_saved);
+  zt_ = st.zt;
+  read_state();
+}
+
 void GpuSolver::scalars(dd* xx, dd* scale, dd* xz, long long* iter) {
   read_state();
   *xx = h_state_.xx;

@@ -78,6 +78,11 @@ class GpuSolver {
   // Raise z_threshold to `z_threshold` and remove the entries with x = 0 and
   // |z scale| <= z_threshold, rebuilding the table; returns the occupied slots.
   unsigned long long compact(double z_threshold);
+  // Checkpoint of the wavefunction and the iteration state (binary file);
+  // loading needs a solver for the same problem, k and m, and a table large
+  // enough for the saved entries, and continues where the saved solve stopped.
+  void checkpoint_save(const std::string& path);
+  void checkpoint_load(const std::string& path);
   // The determinants with x != 0 and their x (scaled: coefficients are scale * x).
   void wavefunction(std::vector<Det>& dets, std::vector<double>& x);
   // Leader-kernel phase timers (SM cycles summed over launches since the last call).
@@ -103,6 +108,7 @@ class GpuSolver {
   void read_state();
   void raise_device_error();
   void build_graph();
+  void gather_slots(double zlim, std::vector<Slot>& out);  // occupied slots kept by zlim, in slot order
 
   SolverOptions opt_;
   HamHost ham_;

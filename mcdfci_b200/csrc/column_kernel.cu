@@ -216,6 +216,16 @@ __device__ __forceinline__ int gen_entry(const HamDev& h, const Prelude& P, int 
   return kIfNonzero;
 }
 
+// |dz scale| > zt, the insertion rule (src/wavefunction.h:517-528): a double
+// product decides unless it lies within 1e-14 of zt, where the
+// double-double product does.
+__device__ __forceinline__ bool above_threshold(dd scale, double dz, double zt) {
+  const double sd = fabs(scale.hi * dz);
+  if (sd > zt * (1.0 + 1e-14)) return true;
+  if (sd < zt * (1.0 - 1e-14)) return false;
+  return dd_gt(dd_abs(dd_mul_d(scale, dz)), dd{zt, 0.0});
+}
+
 __device__ __forceinline__ double score_of(double x, double z, dd xss) {
   if (x == 0.0) return fabs(z);
   const dd t = dd_add_d(dd_mul_d(xss, x), z);
@@ -292,24 +302,18 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
       double v;
       const int kind = gen_entry(L.ham, P, e, hd, a2, b2, v);
       if (kind != kNone) {
-        // Start the probe at the home slot before the integral value is used.
-        const uint64_t home = det_hash(a2, b2) & L.tab.mask;
+        // Start the probe at the home slot before the integral value is used
+        // (the diagonal entry's slot is the picked determinant's own).
+        const uint64_t home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
         uint64_t ka = 0, kb = 0;
-        if (e != 0) load_key(L.tab.slots + home, ka, kb);
+        load_key(L.tab.slots + home, ka, kb);
         if (kind == kKeep || v != 0.0) {
           ++emit;
           const double dz = v * dxc;
-          const bool above = dd_gt(dd_abs(dd_mul_d(scale, dz)), zt);
-          long long slot;
-          if (e == 0) {
-            slot = dslot;
-          } else if (above) {
-            bool inserted;
-            slot = table_upsert_from(L.tab, a2, b2, home, ka, kb, inserted);
-            ins += inserted ? 1u : 0u;
-          } else {
-            slot = table_find_from(L.tab, a2, b2, home, ka, kb);
-          }
+          bool inserted;
+          const long long slot =
+              table_probe_from(L.tab, a2, b2, home, ka, kb, above_threshold(scale, dz, zt.hi), inserted);
+          ins += inserted ? 1u : 0u;
           if (slot >= 0) {
             Slot* sp = L.tab.slots + slot;
             const double x = sp->x;

@@ -158,6 +158,32 @@ __device__ __forceinline__ long long table_find(const TableDev& t, uint64_t a, u
   return table_find_from(t, a, b, i, ka, kb);
 }
 
+// Find, and insert when `insert` (one loop for both, so that the lanes of a
+// warp that insert and those that only update stay on one path), continuing
+// from a loaded home slot as table_find_from.
+__device__ __forceinline__ long long table_probe_from(const TableDev& t, uint64_t a, uint64_t b, uint64_t i,
+                                                      uint64_t ka, uint64_t kb, bool insert, bool& inserted) {
+  inserted = false;
+  for (int p = 0; p < t.max_probe; ++p) {
+    if (p > 0) load_key(t.slots + i, ka, kb);
+    if (ka == a && kb == b) return static_cast<long long>(i);
+    if (ka == kEmptyKey && kb == kEmptyKey) {
+      if (!insert) return -1;
+      uint64_t oa, ob;
+      cas_key(t.slots + i, a, b, oa, ob);
+      if (oa == kEmptyKey && ob == kEmptyKey) {
+        inserted = true;
+        atomicAdd(t.n_occupied, 1ull);
+        return static_cast<long long>(i);
+      }
+      if (oa == a && ob == b) return static_cast<long long>(i);
+    }
+    i = (i + 1) & t.mask;
+  }
+  atomicOr(t.err, kErrProbe);
+  return -1;
+}
+
 // Find or insert, continuing from a loaded home slot as table_find_from.
 // `inserted` is set when this call created the slot (x = z = 0 from the
 // table's initialisation).  Returns -1 only when the probe limit is hit,

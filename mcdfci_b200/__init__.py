@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
+    "mcd_debug_column_sections",
 )
 
 
@@ -137,6 +138,7 @@ def library() -> ctypes.CDLL:
                                         ctypes.POINTER(ctypes.c_int32), vp]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
     L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
+    L.mcd_debug_column_sections.argtypes = [vp, _u64p, ctypes.c_int32, ctypes.c_int32]
     L.mcd_checkpoint_save.argtypes = [vp, ctypes.c_char_p]
     L.mcd_checkpoint_load.argtypes = [vp, ctypes.c_char_p]
     L.mcd_debug_wavefunction.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
@@ -381,6 +383,15 @@ class CDFCI:
         g2 = np.zeros(n ** 4)
         _check(library().mcd_rdm(self._h, g1.ctypes.data_as(_dp), g2.ctypes.data_as(_dp)))
         return g1.reshape(n, n), g2.reshape(n, n, n, n)
+
+    COLUMN_SECTIONS = ("decode", "probe", "update", "offer", "rounds")
+
+    def column_sections(self, enable: bool = True) -> dict:
+        """Column-kernel phase cycles since the previous call; turns the
+        timers on (or off) for later launches."""
+        v = (ctypes.c_uint64 * len(self.COLUMN_SECTIONS))()
+        _check(library().mcd_debug_column_sections(self._h, v, len(v), int(bool(enable))))
+        return dict(zip(self.COLUMN_SECTIONS, list(v)))
 
     def save(self, path: str):
         """Checkpoint of the wavefunction and the iteration state."""

@@ -607,6 +607,15 @@ int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n) {
   });
 }
 
+int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_t enable) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    auto v = s->impl->column_sections(enable != 0);
+    for (int32_t i = 0; cycles && i < n && i < static_cast<int32_t>(v.size()); ++i) cycles[i] = v[i];
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, int32_t* entries) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");

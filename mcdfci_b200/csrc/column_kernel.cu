@@ -293,7 +293,10 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   double acc_newz = 0.0, acc_dot = 0.0;
   unsigned emit = 0, upd = 0, ins = 0;
 
+  const bool timed = L.sect != nullptr && threadIdx.x == 0;
+  unsigned long long t_gen = 0, t_probe = 0, t_upd = 0, t_off = 0;
   for (int r = 0; r < nrounds; ++r) {
+    long long q0 = timed ? clock64() : 0;
     const int e = beg + r * kNT + threadIdx.x;
     unsigned long long key = 0ull;
     unsigned slotu = 0u;
@@ -307,6 +310,11 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
         const uint64_t home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
         uint64_t ka = 0, kb = 0;
         load_key(L.tab.slots + home, ka, kb);
+        long long q1 = 0;
+        if (timed) {
+          q1 = clock64();
+          t_gen += q1 - q0;
+        }
         if (kind == kKeep || v != 0.0) {
           ++emit;
           const double dz = v * dxc;
@@ -314,6 +322,11 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
           const long long slot =
               table_probe_from(L.tab, a2, b2, home, ka, kb, above_threshold(scale, dz, zt.hi), inserted);
           ins += inserted ? 1u : 0u;
+          long long q2 = 0;
+          if (timed) {
+            q2 = clock64();
+            t_probe += q2 - q1;
+          }
           if (slot >= 0) {
             Slot* sp = L.tab.slots + slot;
             const double x = sp->x;
@@ -323,11 +336,21 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
             acc_dot += dz * x;
             key = static_cast<unsigned long long>(__double_as_longlong(score_of(x, znew, xss))) + 1ull;
             slotu = static_cast<unsigned>(slot);
+            if (timed) t_upd += clock64() - q2;
           }
         }
       }
     }
+    const long long q3 = timed ? clock64() : 0;
     toplist_offer<R>(T, key, slotu);
+    if (timed) t_off += clock64() - q3;
+  }
+  if (timed) {
+    atomicAdd(L.sect + 0, t_gen);
+    atomicAdd(L.sect + 1, t_probe);
+    atomicAdd(L.sect + 2, t_upd);
+    atomicAdd(L.sect + 3, t_off);
+    atomicAdd(L.sect + 4, static_cast<unsigned long long>(nrounds));
   }
 
   acc_newz = warp_sum(acc_newz);

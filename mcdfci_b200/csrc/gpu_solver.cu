@@ -307,8 +307,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     d_hsub_ = device_alloc<double>(static_cast<size_t>(kMaxK) * kMaxK, "H_sub");
     d_err_ = device_alloc<unsigned>(1, "error word");
     d_occ_ = device_alloc<unsigned long long>(1, "occupancy");
-    d_sect_ = device_alloc<unsigned long long>(kLeaderSections, "leader timers");
-    check(cudaMemsetAsync(d_sect_, 0, kLeaderSections * sizeof(unsigned long long), stream_), "memset");
+    d_sect_ = device_alloc<unsigned long long>(kLeaderSections + kColumnSections, "phase timers");
+    check(cudaMemsetAsync(d_sect_, 0, (kLeaderSections + kColumnSections) * sizeof(unsigned long long), stream_),
+          "memset");
     const size_t parts = static_cast<size_t>(opt_.k) * groups_;
     d_part_key_ = device_alloc<unsigned long long>(parts * list_, "column partial lists");
     d_part_slot_ = device_alloc<unsigned>(parts * list_, "column partial lists");
@@ -992,6 +993,20 @@ void GpuSolver::table_sums(dd* xx, dd* xz, unsigned long long* occupied) {
   *xx = a;
   *xz = b;
   *occupied = c;
+}
+
+std::vector<unsigned long long> GpuSolver::column_sections(bool enable) {
+  std::vector<unsigned long long> v(kColumnSections);
+  check(cudaStreamSynchronize(stream_), "sync");
+  check(cudaMemcpy(v.data(), d_sect_ + kLeaderSections, v.size() * 8, cudaMemcpyDeviceToHost), "copy");
+  check(cudaMemset(d_sect_ + kLeaderSections, 0, v.size() * 8), "memset");
+  unsigned long long* want = enable ? d_sect_ + kLeaderSections : nullptr;
+  if (cl_.sect != want) {  // the descriptor is recorded in the graph: rebuild it
+    cl_.sect = want;
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  return v;
 }
 
 std::vector<unsigned long long> GpuSolver::leader_sections() {

@@ -87,6 +87,9 @@ class GpuSolver {
   void wavefunction(std::vector<Det>& dets, std::vector<double>& x);
   // Leader-kernel phase timers (SM cycles summed over launches since the last call).
   std::vector<unsigned long long> leader_sections();
+  // Column-kernel phase timers (kColumnSections values since the last call,
+  // which resets them); `enable` turns them on or off for later launches.
+  std::vector<unsigned long long> column_sections(bool enable);
 
   const HamHost& ham() const { return ham_; }
   Det reference_det() const { return ref_; }

@@ -74,6 +74,7 @@ struct ColumnLaunch {
   unsigned* part_slot;           // [kMaxK][groups][list]
   double* part_sum;              // [kMaxK][groups][2] per-CTA new_z and dot partial sums
   unsigned* done;                // [kMaxK] CTAs finished per column (reset by the last one)
+  unsigned long long* sect;  // [kColumnSections] SM cycles per phase of thread 0's rounds, or null
   int m;
   int groups;             // CTAs per column
   int k_grid;             // columns launched (>= k_cur)
@@ -131,6 +132,11 @@ struct RdmLaunch {
 // 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
 // 15 eig finish.
 constexpr int kLeaderSections = 16;
+
+// Phases of the column kernel timed into ColumnLaunch::sect (thread 0 of each
+// CTA, summed): 0 entry decode and integral value, 1 slot probe, 2 x load,
+// z atomic and score, 3 candidate offer, 4 rounds counted.
+constexpr int kColumnSections = 5;
 
 // Launchers (column_kernel.cu / leader_kernel.cu).
 int column_entries(int norb, int na, int nb);

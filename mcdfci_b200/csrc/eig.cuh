@@ -5,12 +5,14 @@
 // step of __float128 inverse iteration through dgetrf (src/solver.h:400-503).
 // Here the work is arranged around the serial dependencies of one CTA:
 //   1. Householder reduction to tridiagonal T = Q^T A Q (Golub & Van Loan,
-//      Algorithm 8.3.1) by four warps per 32 rows, one pass over the trailing
-//      rows per step: the next pivot row is updated first, one column per
-//      thread, every thread derives the next reflector from its norm, and
-//      then the trailing rows, each split over four lanes, are updated with
-//      reflector j while p = tau A u for reflector j+1 is formed.  Reflector
-//      j is H_j = I - tau_j u_j u_j^T with u_j = (0..0, A[j][j+1..n)), where
+//      Algorithm 8.3.1).  Up to 33 rows (k <= 32) one warp holds the matrix
+//      in registers, a row per lane, and needs no CTA barrier; larger
+//      matrices take four warps per 32 rows, one pass over the trailing rows
+//      per step: the next pivot row is updated first, one column per thread,
+//      every thread derives the next reflector from its norm, and then the
+//      trailing rows, each split over four lanes, are updated with reflector
+//      j while p = tau A u for reflector j+1 is formed.  Reflector j is
+//      H_j = I - tau_j u_j u_j^T with u_j = (0..0, A[j][j+1..n)), where
 //      A[j][j+1] holds u0_j; row j is not written after step j.
 //   2. The lowest eigenvalue of T is bracketed by 128-way multisection on four
 //      warps (one per SM sub-partition): T - sigma I is positive definite
@@ -35,7 +37,7 @@
 
 namespace mcd {
 
-constexpr int kEigThreads = 1024;
+constexpr int kEigThreads = 512;
 constexpr int kEigBracketWarps = 4;
 constexpr int kEigBracketRounds = 5;  // 129^5 = 3.6e10 : 1 reduction of the Gershgorin interval
 
@@ -272,6 +274,99 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
   }
 }
 
+// Rows of the largest matrix that the one-warp reduction takes.
+constexpr int kEigWarpRows = 33;
+
+// a[j] for a register array and a run-time j in [0, 33): a tree of selects
+// on the bits of j, so that a stays in registers.
+__device__ __forceinline__ double reg_pick33(const double (&a)[kEigWarpRows], int j) {
+  double t[16];
+  const bool b0 = (j & 1) != 0, b1 = (j & 2) != 0, b2 = (j & 4) != 0, b3 = (j & 8) != 0, b4 = (j & 16) != 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) t[i] = b0 ? a[2 * i + 1] : a[2 * i];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) t[i] = b1 ? t[2 * i + 1] : t[2 * i];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) t[i] = b2 ? t[2 * i + 1] : t[2 * i];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) t[i] = b3 ? t[2 * i + 1] : t[2 * i];
+  t[0] = b4 ? t[1] : t[0];
+  return j >= 32 ? a[32] : t[0];
+}
+
+// 1 (one warp).  Tridiagonalisation of an n x n matrix, 3 <= n <= 33, by
+// warp 0 with lane l holding row l+1 in registers (row 0 is only read: A[0][0]
+// is d_0, and every reflector acts on indices 1..n-1).  Step j: column j of
+// the rows below the diagonal is a register picked by j; one warp sum gives
+// reflector j (every lane derives the same scalars: a butterfly sum gives all
+// lanes the same value), u is broadcast through shared memory, p = tau A u
+// and K = tau/2 p'u follow with one more warp sum, and the rank-2 update
+// A -= u w' + w u' (w = p - K u) reads u and w two elements per load.  Rows
+// and columns up to j keep w = 0 and u = 0, so the finished part of the
+// register matrix no longer changes.  Same outputs as eig_tridiag.
+__device__ __forceinline__ void eig_tridiag_warp(double* A, int lda, int n, const EigVecs& V) {
+  constexpr int NC = kEigWarpRows;
+  __shared__ __align__(16) double s_u[NC + 1];
+  __shared__ __align__(16) double s_w[NC + 1];
+  const int lane = threadIdx.x & 31;
+  const int r = lane + 1;
+  const bool live = r < n;
+  double a[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) a[c] = (live && c < n) ? A[r * lda + c] : 0.0;
+  if (lane == 0) {
+    V.d[0] = A[0];
+    s_u[0] = s_u[NC] = 0.0;
+    s_w[0] = s_w[NC] = 0.0;
+  }
+  const double2* u2 = reinterpret_cast<const double2*>(s_u);
+  const double2* w2 = reinterpret_cast<const double2*>(s_w);
+  for (int j = 0; j + 2 < n; ++j) {
+    const double x = reg_pick33(a, j);  // A[r][j]
+    if (j >= 1 && lane == j - 1) V.d[j] = x;  // row j is final after step j-1
+    const double s = warp_sum((live && r >= j + 2) ? x * x : 0.0);
+    const double x0 = __shfl_sync(~0u, x, j);  // A[j+1][j]
+    double u0, tau, e;
+    eig_reflector(x0, s, u0, tau, e);
+    const bool act = live && r >= j + 1;
+    const double ur = !act ? 0.0 : (r == j + 1 ? u0 : x);
+    s_u[r] = ur;
+    if (act) A[j * lda + r] = ur;
+    if (lane == 0) {
+      V.e[j] = e;
+      V.u0[j] = u0;
+      V.tau[j] = tau;
+    }
+    __syncwarp();
+    double pa[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c2 = 0; c2 <= NC / 2; ++c2) {
+      const double2 u = u2[c2];
+      pa[c2 & 3] = fma(a[2 * c2], u.x, pa[c2 & 3]);
+      if (2 * c2 + 1 < NC) pa[c2 & 3] = fma(a[2 * c2 + 1], u.y, pa[c2 & 3]);
+    }
+    const double p = tau * ((pa[0] + pa[1]) + (pa[2] + pa[3]));
+    const double K = 0.5 * tau * warp_sum(ur * p);
+    const double wr = act ? fma(-K, ur, p) : 0.0;
+    s_w[r] = wr;
+    __syncwarp();
+#pragma unroll
+    for (int c2 = 0; c2 <= NC / 2; ++c2) {
+      const double2 u = u2[c2], w = w2[c2];
+      a[2 * c2] = fma(-ur, w.x, fma(-wr, u.x, a[2 * c2]));
+      if (2 * c2 + 1 < NC) a[2 * c2 + 1] = fma(-ur, w.y, fma(-wr, u.y, a[2 * c2 + 1]));
+    }
+    __syncwarp();  // s_u and s_w are rewritten by the next step
+  }
+  const double y = reg_pick33(a, n - 2);
+  const double z = reg_pick33(a, n - 1);
+  if (lane == n - 3) V.d[n - 2] = y;
+  if (lane == n - 2) {
+    V.e[n - 2] = y;  // A[n-1][n-2]
+    V.d[n - 1] = z;
+  }
+}
+
 // Rescales a pair of consecutive minors by a power of two when the newer one
 // leaves [1e-150, 1e150]; signs and the ratio are unchanged.  Called every
 // four recurrence steps, which grow the magnitudes by far less than 1e150.
@@ -500,7 +595,11 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
     __syncthreads();
     return;
   }
-  if (warp < eig_tridiag_warps(n)) eig_tridiag(A, lda, n, V);
+  if (n >= 3 && n <= kEigWarpRows) {
+    if (warp == 0) eig_tridiag_warp(A, lda, n, V);
+  } else if (warp < eig_tridiag_warps(n)) {
+    eig_tridiag(A, lda, n, V);
+  }
   __syncthreads();
   clk.mark(10);
 
@@ -517,7 +616,7 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
 
   // 4. Back-transformation.
   double* y = V.y;
-  for (int j = warp; j < n - 2; j += 32) {
+  for (int j = warp; j < n - 2; j += kEigThreads / 32) {
     const double* rj = A + j * lda;
     double s = 0.0;
     for (int c = j + 2 + lane; c < n; c += 32) s = fma(rj[c], y[c], s);
@@ -561,7 +660,7 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
     }
   }
   __syncthreads();
-  for (int r = warp; r < n; r += 32) {
+  for (int r = warp; r < n; r += kEigThreads / 32) {
     const int jmax = min(r - 1, n - 3);
     double s = 0.0;
     for (int j = lane; j <= jmax; j += 32) {

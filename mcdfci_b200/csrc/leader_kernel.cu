@@ -27,12 +27,12 @@
 #include "eig.cuh"
 #include "device_common.cuh"
 #include "kernels.h"
-#include "toplist.cuh"
 
 namespace mcd {
 namespace {
 
-constexpr int kLT = kEigThreads;  // 1024
+constexpr int kLT = kEigThreads;  // 512
+constexpr int kLW = kLT / 32;     // warps
 
 // ---------------------------------------------------------------------------
 // Matrix elements between two determinants.
@@ -208,7 +208,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   __syncthreads();
   // H x in double (dsymv, src/solver.h:355); x'x, x'z, x'Hx in double-double,
   // rounded where the reference works in double.
-  for (int r = warp; r < k; r += 32) {
+  for (int r = warp; r < k; r += kLW) {
     const double* row = A + (r + 1) * lda + 1;
     double s = 0.0;
     for (int c = lane; c < k; c += 32) s = fma(row[c], x[c], s);
@@ -260,7 +260,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
 
   // B v in double, one row per warp (H is symmetric, so its rows are read).
   const double* y = V.y;
-  for (int r = warp; r < n; r += 32) {
+  for (int r = warp; r < n; r += kLW) {
     double s = 0.0;
     if (branch == 1) {
       const double* hr = H + (r - 1) * k - 1;  // hr[c] = H[r-1][c-1]
@@ -407,39 +407,125 @@ __device__ __forceinline__ int block_rank(bool keep, int* wsum, int* chunk_total
 constexpr unsigned kNoSlot = 0xFFFFFFFFu;
 
 // The k best (score, slot) pairs among n candidates (us, sc in shared
-// memory), k < 32R.  Each warp keeps a top-32R list of its share; the lists
-// merge as a tree in `scratch` (which may alias us and sc: it is written only
-// after every warp has read them).  Writes the k slots in order of decreasing
-// score and returns false when the k-th and (k+1)-th scores are equal, so that
-// the caller can order that tie by determinant.
-template <int R>
-__device__ bool topk_fast(const unsigned* us, const double* sc, int n, int k, unsigned char* scratch,
-                          unsigned* out) {
-  __shared__ int s_tie;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  TopList<R> T;
-  toplist_clear<R>(T);
+// memory) by radix selection on the 64-bit keys bits(score) + 1: scores are
+// +0 or positive, so their bit patterns order like their values.  Eight-bit
+// digits from the top, one 256-bin shared histogram per pass (warp-aggregated
+// counts: the leading digits of nearby scores coincide), until the bin that
+// holds the k-th largest key holds exactly the keys still to choose.  The
+// chosen keys are then ranked among themselves, in decreasing score and equal
+// scores in the reference's determinant order (detComp_global,
+// src/wavefunction.h:30-36), and their slots written to out[0..k) in that
+// order.  Returns false, writing nothing, when the k-th and (k+1)-th keys are
+// equal, so that the caller can choose the set by determinant order.
+__device__ bool topk_radix(const unsigned* us, const double* sc, int n, int k, const Slot* slots, int nwords,
+                           unsigned* out) {
+  __shared__ unsigned s_hist[256];
+  __shared__ unsigned long long s_sel_key[kMaxK];
+  __shared__ unsigned s_sel_slot[kMaxK];
+  __shared__ unsigned long long s_prefix;
+  __shared__ unsigned s_need;
+  __shared__ int s_state, s_count;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < 256) s_hist[tid] = 0u;
+  if (tid == 0) {
+    s_need = static_cast<unsigned>(k);
+    s_count = 0;
+    s_state = 0;
+    s_prefix = 0ull;
+  }
+  __syncthreads();
+  unsigned long long prefix = 0ull;  // the digits chosen so far, lower bits 0
+  int state = 0;                     // 0 more digits, 1 set found, 2 tie at the k-th key
+  for (int pass = 0; pass < 8 && state == 0; ++pass) {
+    const int shift = 56 - 8 * pass;
+    const unsigned long long himask = pass == 0 ? 0ull : (~0ull << (shift + 8));
+    for (int base = warp * 32; base < n; base += blockDim.x) {
+      const int u = base + lane;
+      const unsigned long long key =
+          u < n ? static_cast<unsigned long long>(__double_as_longlong(sc[u])) + 1ull : 0ull;
+      const bool match = u < n && ((key ^ prefix) & himask) == 0ull;
+      const unsigned act = __ballot_sync(~0u, match);
+      if (match) {
+        const unsigned d = static_cast<unsigned>(key >> shift) & 255u;
+        const unsigned peers = __match_any_sync(act, d);
+        if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[d], static_cast<unsigned>(__popc(peers)));
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // Lane l holds bins 255-8l .. 248-8l, in decreasing order.
+      const unsigned need = s_need;
+      unsigned c[8], t = 0u;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        c[j] = s_hist[255 - 8 * lane - j];
+        s_hist[255 - 8 * lane - j] = 0u;
+        t += c[j];
+      }
+      unsigned incl = t;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(~0u, incl, o);
+        if (lane >= o) incl += v;
+      }
+      unsigned run = incl - t;  // keys in higher bins
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (run < need && run + c[j] >= need) {
+          const unsigned long long d = static_cast<unsigned long long>(255 - 8 * lane - j);
+          s_prefix = prefix | (d << shift);
+          s_need = need - run;
+          s_state = (c[j] == need - run) ? 1 : (pass == 7 ? 2 : 0);
+        }
+        run += c[j];
+      }
+    }
+    __syncthreads();
+    prefix = s_prefix;
+    state = s_state;
+  }
+  if (state != 1) return false;
+  // The chosen keys are those >= prefix: exactly k of them.
   for (int base = warp * 32; base < n; base += blockDim.x) {
     const int u = base + lane;
     const unsigned long long key =
         u < n ? static_cast<unsigned long long>(__double_as_longlong(sc[u])) + 1ull : 0ull;
-    toplist_offer<R>(T, key, u < n ? us[u] : 0u);
-  }
-  __syncthreads();
-  unsigned long long* skey = reinterpret_cast<unsigned long long*>(scratch);
-  unsigned* spay = reinterpret_cast<unsigned*>(skey + (blockDim.x >> 5) * 32 * R);
-  toplist_cta_merge<R>(T, skey, spay);
-  if (warp == 0) {
-#pragma unroll
-    for (int j = 0; j < R; ++j)
-      if (j * 32 + lane < k) out[j * 32 + lane] = T.p[j];
-    if (lane == 0) {
-      const unsigned long long a = skey[k - 1], b = skey[k];
-      s_tie = (b != 0ull && a == b) ? 1 : 0;
+    const bool keep = u < n && key >= prefix;
+    const unsigned b = __ballot_sync(~0u, keep);
+    if (b == 0u) continue;
+    int pos = 0;
+    if (lane == 0) pos = atomicAdd(&s_count, __popc(b));
+    pos = __shfl_sync(~0u, pos, 0) + __popc(b & lanemask_lt());
+    if (keep) {
+      s_sel_key[pos] = key;
+      s_sel_slot[pos] = us[u];
     }
   }
   __syncthreads();
-  return s_tie == 0;
+  if (tid < k) {
+    const unsigned long long mine = s_sel_key[tid];
+    const unsigned slot = s_sel_slot[tid];
+    int rank = 0;
+    bool equal = false;
+    for (int j = 0; j < k; ++j) {
+      const unsigned long long o = s_sel_key[j];
+      rank += o > mine;
+      equal |= (o == mine) && j != tid;
+    }
+    if (equal) {  // equal scores: the reference's determinant order
+      uint64_t ia, ib;
+      load_key(slots + slot, ia, ib);
+      for (int j = 0; j < k; ++j) {
+        if (j == tid || s_sel_key[j] != mine) continue;
+        uint64_t ja, jb;
+        load_key(slots + s_sel_slot[j], ja, jb);
+        rank += det_ref_compare(ja, jb, ia, ib, nwords) > 0;
+      }
+    }
+    out[rank] = slot;
+  }
+  __syncthreads();
+  return true;
 }
 
 
@@ -453,7 +539,7 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   __shared__ unsigned s_slot[kMaxK];
   __shared__ Det s_det[kMaxK];
   __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
-  __shared__ unsigned char s_occ[32][128];
+  __shared__ unsigned char s_occ[kLW][128];
   __shared__ unsigned long long s_newx;
 
   IterState* G = L.st;
@@ -523,55 +609,86 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   double* sc = reinterpret_cast<double*>(hs);
   const int H = 2 * PR;
   const dd xss = sS.xss;
+  auto slot_of = [&](int r) {  // candidate r: s_off[lo] <= r < s_off[lo+1]
+    int lo = 0, hi = kprev;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s_off[mid] <= r) lo = mid; else hi = mid;
+    }
+    return L.cand_slot[lo * m + (r - s_off[lo])];
+  };
+  auto score_at = [&](unsigned slot) {
+    const Slot* sp = T.slots + slot;
+    const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
+    const double g = score_of(x, z, xss);
+    return (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the padding
+  };
+  auto hash_keep = [&](unsigned s) {  // true for the first copy of slot s
+    unsigned h = hash32(s) & static_cast<unsigned>(H - 1);
+    for (int probe = 0; probe < H; ++probe) {
+      const unsigned old = atomicCAS(&hs[h], kNoSlot, s);
+      if (old == kNoSlot) return true;
+      if (old == s) return false;
+      h = (h + 1) & static_cast<unsigned>(H - 1);
+    }
+    return false;
+  };
+  // With at most two candidates per thread (the usual case), each thread
+  // fetches its candidates' slots and scores in one go, before the duplicate
+  // removal, and the scores are written once the hash set is done with.
   auto gather = [&]() {
     for (int i = tid; i < H; i += kLT) hs[i] = kNoSlot;
-    for (int r = tid; r < R; r += kLT) {
-      int lo = 0, hi = kprev;  // s_off[lo] <= r < s_off[lo+1]
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_off[mid] <= r) lo = mid; else hi = mid;
-      }
-      us[r] = L.cand_slot[lo * m + (r - s_off[lo])];
-    }
-    __syncthreads();
     int total = 0;
-    for (int base = 0; base < R; base += kLT) {
-      const int r = base + tid;
-      const unsigned s = r < R ? us[r] : kNoSlot;
-      bool keep = false;
-      if (r < R) {
-        unsigned h = hash32(s) & static_cast<unsigned>(H - 1);
-        for (int probe = 0; probe < H; ++probe) {
-          const unsigned old = atomicCAS(&hs[h], kNoSlot, s);
-          if (old == kNoSlot) {
-            keep = true;
-            break;
-          }
-          if (old == s) break;
-          h = (h + 1) & static_cast<unsigned>(H - 1);
-        }
-      }
-      int chunk = 0;
-      const int pos = block_rank(keep, s_wsum, &chunk);
-      if (keep) us[total + pos] = s;
-      total += chunk;
+    if (R <= 2 * kLT) {
+      const int r0 = tid, r1 = kLT + tid;
+      const unsigned s0 = r0 < R ? slot_of(r0) : kNoSlot;
+      const unsigned s1 = r1 < R ? slot_of(r1) : kNoSlot;
+      const double g0 = r0 < R ? score_at(s0) : 0.0;
+      const double g1 = r1 < R ? score_at(s1) : 0.0;
       __syncthreads();
+      int p0 = -1, p1 = -1, chunk = 0;
+      bool keep = r0 < R && hash_keep(s0);
+      int pos = block_rank(keep, s_wsum, &chunk);
+      if (keep) {
+        us[pos] = s0;
+        p0 = pos;
+      }
+      total = chunk;
+      __syncthreads();
+      if (R > kLT) {
+        keep = r1 < R && hash_keep(s1);
+        pos = block_rank(keep, s_wsum, &chunk);
+        if (keep) {
+          us[total + pos] = s1;
+          p1 = total + pos;
+        }
+        total += chunk;
+        __syncthreads();
+      }
+      // The hash set (which sc overlays) is no longer read.
+      if (p0 >= 0) sc[p0] = g0;
+      if (p1 >= 0) sc[p1] = g1;
+    } else {
+      for (int r = tid; r < R; r += kLT) us[r] = slot_of(r);
+      __syncthreads();
+      for (int base = 0; base < R; base += kLT) {
+        const int r = base + tid;
+        const unsigned s = r < R ? us[r] : kNoSlot;
+        const bool keep = r < R && hash_keep(s);
+        int chunk = 0;
+        const int pos = block_rank(keep, s_wsum, &chunk);
+        if (keep) us[total + pos] = s;
+        total += chunk;
+        __syncthreads();
+      }
+      for (int u = tid; u < total; u += kLT) sc[u] = score_at(us[u]);
     }
     if (tid == 0) s_U = total;
-    __syncthreads();
-    const int Ul = s_U;
     int Pl = 1;
-    while (Pl < Ul) Pl <<= 1;
-    for (int u = tid; u < Pl; u += kLT) {
-      if (u < Ul) {
-        const Slot* sp = T.slots + us[u];
-        const double x = load_relaxed(&sp->x), z = load_relaxed(&sp->z);
-        const double g = score_of(x, z, xss);
-        sc[u] = (g >= 0.0) ? g : 0.0;  // a non-finite gradient must not reorder the padding
-      } else {
-        sc[u] = -1.0;
-        us[u] = kNoSlot;
-      }
+    while (Pl < total) Pl <<= 1;
+    for (int u = total + tid; u < Pl; u += kLT) {
+      sc[u] = -1.0;
+      us[u] = kNoSlot;
     }
     __syncthreads();
   };
@@ -580,20 +697,12 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   const int U = s_U;
   const int k = U < L.k_req ? U : L.k_req;
 
-  // 4. The k largest scores: per-warp top lists over the candidates, merged
-  //    as a tree.  Equal scores are ordered by the reference's determinant
-  //    order (detComp_global, src/wavefunction.h:30-36); when the k-th and
-  //    (k+1)-th scores are equal that order decides the set, and the whole
-  //    candidate list is sorted instead (rare).
-  bool fast;
-  if (k < 32)
-    fast = topk_fast<1>(us, sc, U, k, smem, s_slot);
-  else if (k < 64)
-    fast = topk_fast<2>(us, sc, U, k, smem, s_slot);
-  else if (k < 128)
-    fast = topk_fast<4>(us, sc, U, k, smem, s_slot);
-  else
-    fast = topk_fast<8>(us, sc, U, k, smem, s_slot);
+  // 4. The k largest scores, by radix selection over the candidates.  Equal
+  //    scores are ordered by the reference's determinant order
+  //    (detComp_global, src/wavefunction.h:30-36); when the k-th and (k+1)-th
+  //    scores are equal that order decides the set, and the whole candidate
+  //    list is sorted instead (rare).
+  const bool fast = topk_radix(us, sc, U, k, T.slots, sS.n_words, s_slot);
   clk.mark(3);
   if (!fast) {
     gather();
@@ -652,15 +761,17 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   const bool h_in_smem = k <= 64;
   double* Hs = h_in_smem ? reinterpret_cast<double*>(smem) : L.hsub_out;
   double* work = h_in_smem ? Hs + k * k : reinterpret_cast<double*>(smem);
-  for (int t = tid; t < k * k; t += kLT) {
-    const int i = t / k, j = t - i * k;
-    if (i < j) {
-      const double v = off_diagonal(L.ham, s_det[i], s_det[j]);
-      Hs[i * k + j] = v;
-      Hs[j * k + i] = v;
-    }
+  // One thread per pair i < j (pair t = j(j-1)/2 + i).
+  for (int t = tid; t < k * (k - 1) / 2; t += kLT) {
+    int j = static_cast<int>((1.0f + sqrtf(1.0f + 8.0f * static_cast<float>(t))) * 0.5f);
+    while (j * (j - 1) / 2 > t) --j;
+    while (j * (j + 1) / 2 <= t) ++j;
+    const int i = t - j * (j - 1) / 2;
+    const double v = off_diagonal(L.ham, s_det[i], s_det[j]);
+    Hs[i * k + j] = v;
+    Hs[j * k + i] = v;
   }
-  for (int i = warp; i < k; i += 32) {
+  for (int i = warp; i < k; i += kLW) {
     const double v = diagonal_warp(L.ham, s_det[i], s_occ[warp]);
     if (lane == 0) Hs[i * k + i] = v;
   }
@@ -768,7 +879,7 @@ __global__ void init_kernel(LeaderLaunch L, Det ref, double ref_diag) {
 }
 
 __global__ void debug_hsub_kernel(HamDev h, const Det* dets, int k, double* H) {
-  __shared__ unsigned char s_occ[32][128];
+  __shared__ unsigned char s_occ[kLW][128];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int t = tid; t < k * k; t += blockDim.x) {
     const int i = t / k, j = t - i * k;
@@ -816,9 +927,7 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, con
 size_t leader_smem_bytes(int k, int m) {
   size_t P = 2;
   while (P < static_cast<size_t>(k) * m) P <<= 1;
-  size_t pick = P * 4 + 2 * P * 4;  // slots + hash set (the hash set area later holds P doubles)
-  const size_t lists = static_cast<size_t>(kLT / 32) * 32 * (k < 32 ? 1 : k < 64 ? 2 : k < 128 ? 4 : 8) * 12;
-  if (lists > pick) pick = lists;  // top-k merge scratch, aliasing the candidate arrays
+  const size_t pick = P * 4 + 2 * P * 4;  // slots + hash set (the hash set area later holds P doubles)
   const size_t hs = (k <= 64 ? static_cast<size_t>(k) * k : 0) * sizeof(double);
   const size_t eig = hs + eig_work_doubles(k) * sizeof(double);
   return pick > eig ? pick : eig;

@@ -272,11 +272,14 @@ int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n);
 /* The determinants with nonzero x and their x (the coefficients are scale * x),
  * sorted by slot; up to cap of them, *n_out receives the count. */
 int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, int64_t cap, int64_t* n_out);
-/* SM cycles of thread 0 of every column-kernel CTA in each phase of its
- * rounds (5 values: entry decode and integral value, slot probe, x load, z
- * atomic and score, candidate offer; then the number of rounds), summed since
- * the previous call, which resets them; enable = 1 turns the timers on for
- * later launches, 0 off (the default).  No counterpart in the reference. */
+/* SM cycles of thread 0 of every column-kernel CTA in each phase (10
+ * values: per round entry decode and integral value, slot probe, x load, z
+ * atomic and score, candidate offer; the number of rounds; per CTA the
+ * prelude before the first round, the CTA list merge, store and ticket, the
+ * column's final merge by its last CTA; the number of CTAs and of final
+ * merges), summed since the previous call, which resets them; enable = 1
+ * turns the timers on for later launches, 0 off (the default).  No
+ * counterpart in the reference. */
 int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_t enable);
 /* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);

@@ -384,7 +384,7 @@ class CDFCI:
         _check(library().mcd_rdm(self._h, g1.ctypes.data_as(_dp), g2.ctypes.data_as(_dp)))
         return g1.reshape(n, n), g2.reshape(n, n, n, n)
 
-    COLUMN_SECTIONS = ("decode", "probe", "update", "offer", "rounds")
+    COLUMN_SECTIONS = ("decode", "probe", "update", "offer", "rounds", "prelude", "post", "merge", "ctas", "merges")
 
     def column_sections(self, enable: bool = True) -> dict:
         """Column-kernel phase cycles since the previous call; turns the

@@ -273,6 +273,8 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   __shared__ int s_last;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool timed = L.sect != nullptr && threadIdx.x == 0;
+  const long long c_start = timed ? clock64() : 0;
   if (warp == 0) build_prelude(P, S->det[col], L.ham.norb);
   __syncthreads();
 
@@ -293,8 +295,8 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   double acc_newz = 0.0, acc_dot = 0.0;
   unsigned emit = 0, upd = 0, ins = 0;
 
-  const bool timed = L.sect != nullptr && threadIdx.x == 0;
   unsigned long long t_gen = 0, t_probe = 0, t_upd = 0, t_off = 0;
+  const long long c_rounds = timed ? clock64() : 0;
   for (int r = 0; r < nrounds; ++r) {
     long long q0 = timed ? clock64() : 0;
     const int e = beg + r * kNT + threadIdx.x;
@@ -345,12 +347,15 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
     toplist_offer<R>(T, key, slotu);
     if (timed) t_off += clock64() - q3;
   }
+  const long long c_post = timed ? clock64() : 0;
   if (timed) {
     atomicAdd(L.sect + 0, t_gen);
     atomicAdd(L.sect + 1, t_probe);
     atomicAdd(L.sect + 2, t_upd);
     atomicAdd(L.sect + 3, t_off);
     atomicAdd(L.sect + 4, static_cast<unsigned long long>(nrounds));
+    atomicAdd(L.sect + 5, static_cast<unsigned long long>(c_rounds - c_start));
+    atomicAdd(L.sect + 8, 1ull);
   }
 
   acc_newz = warp_sum(acc_newz);
@@ -397,6 +402,8 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   __syncthreads();
   if (threadIdx.x == 0) s_last = (atomicAdd(L.done + col, 1u) == static_cast<unsigned>(G - 1));
   __syncthreads();
+  const long long c_merge = timed ? clock64() : 0;
+  if (timed) atomicAdd(L.sect + 6, static_cast<unsigned long long>(c_merge - c_post));
   if (!s_last) return;
   __threadfence();
 
@@ -433,6 +440,10 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
       S->cand_n[col] = n;
       L.done[col] = 0u;
     }
+  }
+  if (timed) {
+    atomicAdd(L.sect + 7, static_cast<unsigned long long>(clock64() - c_merge));
+    atomicAdd(L.sect + 9, 1ull);
   }
 }
 

@@ -5,10 +5,10 @@
 // step of __float128 inverse iteration through dgetrf (src/solver.h:400-503).
 // Here the work is arranged around the serial dependencies of one CTA:
 //   1. Householder reduction to tridiagonal T = Q^T A Q (Golub & Van Loan,
-//      Algorithm 8.3.1).  Up to 33 rows (k <= 32) one warp holds the matrix
-//      in registers, a row per lane, and needs no CTA barrier; larger
-//      matrices take four warps per 32 rows, one pass over the trailing rows
-//      per step: the next pivot row is updated first, one column per thread,
+//      Algorithm 8.3.1).  Up to 33 rows (k <= 32) four warps hold the
+//      matrix in registers, a row per four lanes, two barriers per step;
+//      larger matrices take four warps per 32 rows in shared memory, one
+//      pass over the trailing rows per step: the next pivot row is updated first, one column per thread,
 //      every thread derives the next reflector from its norm, and then the
 //      trailing rows, each split over four lanes, are updated with reflector
 //      j while p = tau A u for reflector j+1 is formed.  Reflector j is
@@ -20,8 +20,10 @@
 //      the minors follow p_{i+1} = (d_i - sigma) p_i - e_{i-1}^2 p_{i-1}.
 //      Meanwhile the other warps form M[i][j] = tau_i u_j^T u_i (j < i) in
 //      the lower triangle of A, which the reduction no longer reads.
-//   3. Inverse iteration on T - sigma I with sigma at the lower end of the
-//      bracket (positive definite, so LU without pivoting is stable).  The LU
+//   3. Two steps of inverse iteration on T - sigma I with sigma at the lower
+//      end of the bracket (positive definite, so LU without pivoting is
+//      stable); the bracket is 2.8e-11 of the Gershgorin interval wide, so each
+//      step shrinks the other eigenvectors' share by that over the gap.  The LU
 //      pivots are the ratios p_{i+1}/p_i of the same minors: one FMA
 //      recurrence, then independent divisions.
 //   4. Back-transformation v = H_0 H_1 ... H_{n-3} y without a chain of
@@ -39,6 +41,7 @@ namespace mcd {
 
 constexpr int kEigThreads = 512;
 constexpr int kEigBracketWarps = 4;
+constexpr int kEigInverseSteps = 2;  // inverse-iteration steps from the bracket's lower end
 constexpr int kEigBracketRounds = 5;  // 129^5 = 3.6e10 : 1 reduction of the Gershgorin interval
 
 // Leading dimension of an n x n work matrix: odd, so that the lanes of a warp
@@ -274,97 +277,166 @@ __device__ __forceinline__ void eig_tridiag(double* A, int lda, int n, const Eig
   }
 }
 
-// Rows of the largest matrix that the one-warp reduction takes.
-constexpr int kEigWarpRows = 33;
+// Rows of the largest matrix that the register reduction takes.
+constexpr int kEigRegRows = 33;
 
-// a[j] for a register array and a run-time j in [0, 33): a tree of selects
-// on the bits of j, so that a stays in registers.
-__device__ __forceinline__ double reg_pick33(const double (&a)[kEigWarpRows], int j) {
-  double t[16];
-  const bool b0 = (j & 1) != 0, b1 = (j & 2) != 0, b2 = (j & 4) != 0, b3 = (j & 8) != 0, b4 = (j & 16) != 0;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) t[i] = b0 ? a[2 * i + 1] : a[2 * i];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) t[i] = b1 ? t[2 * i + 1] : t[2 * i];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) t[i] = b2 ? t[2 * i + 1] : t[2 * i];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) t[i] = b3 ? t[2 * i + 1] : t[2 * i];
-  t[0] = b4 ? t[1] : t[0];
-  return j >= 32 ? a[32] : t[0];
+// eig_reflector without branches (s == 0 selects H = I), so that its two
+// square roots can be scheduled together with independent work.
+__device__ __forceinline__ void eig_reflector_nb(double x0, double s, double& u0, double& tau, double& e) {
+  const bool none = s == 0.0;
+  const double q = none ? 1.0 : fma(x0, x0, s);
+  const double mu = q * rsqrt(q);
+  const double sg = x0 < 0.0 ? -1.0 : 1.0;
+  const double uu = fma(sg, mu, x0);
+  const double r = rsqrt(mu * fabs(uu));
+  u0 = none ? 0.0 : uu;
+  tau = none ? 0.0 : r * r;
+  e = none ? x0 : -sg * mu;
 }
 
-// 1 (one warp).  Tridiagonalisation of an n x n matrix, 3 <= n <= 33, by
-// warp 0 with lane l holding row l+1 in registers (row 0 is only read: A[0][0]
-// is d_0, and every reflector acts on indices 1..n-1).  Step j: column j of
-// the rows below the diagonal is a register picked by j; one warp sum gives
-// reflector j (every lane derives the same scalars: a butterfly sum gives all
-// lanes the same value), u is broadcast through shared memory, p = tau A u
-// and K = tau/2 p'u follow with one more warp sum, and the rank-2 update
-// A -= u w' + w u' (w = p - K u) reads u and w two elements per load.  Rows
-// and columns up to j keep w = 0 and u = 0, so the finished part of the
-// register matrix no longer changes.  Same outputs as eig_tridiag.
-__device__ __forceinline__ void eig_tridiag_warp(double* A, int lda, int n, const EigVecs& V) {
-  constexpr int NC = kEigWarpRows;
-  __shared__ __align__(16) double s_u[NC + 1];
-  __shared__ __align__(16) double s_w[NC + 1];
-  const int lane = threadIdx.x & 31;
-  const int r = lane + 1;
+// a[i] for a register array of nine and a run-time i in [0, 9): a tree of
+// selects on the bits of i, so that a stays in registers.
+__device__ __forceinline__ double reg_pick9(const double (&a)[9], int i) {
+  const bool b0 = (i & 1) != 0, b1 = (i & 2) != 0, b2 = (i & 4) != 0;
+  const double t0 = b0 ? a[1] : a[0], t1 = b0 ? a[3] : a[2];
+  const double t2 = b0 ? a[5] : a[4], t3 = b0 ? a[7] : a[6];
+  const double s0 = b1 ? t1 : t0, s1 = b1 ? t3 : t2;
+  return i >= 8 ? a[8] : (b2 ? s1 : s0);
+}
+
+// Shared-memory index of column c in the per-quarter vectors: quarter q
+// (columns 9q .. 9q+8) starts at 10q, 16-byte aligned.
+__device__ __forceinline__ int qpos(int c) { return c + c / 9; }
+
+// 1 (registers).  Tridiagonalisation of an n x n matrix, 3 <= n <= 33, by
+// four warps (one per SM sub-partition) holding the matrix in registers:
+// row r = 1..32 belongs to the four lanes 4(r-1)..4(r-1)+3, lane quarter q
+// keeping columns 9q..9q+8 (row 0 is only read: A[0][0] is d_0 and every
+// reflector acts on indices 1..n-1).  Step j, two barriers:
+//   (a) column j (a register picked by j, shuffled within the row) is
+//       published, zero in the finished rows, together with row j+1 and each
+//       warp's partial of the column's squared norm;
+//   (b) every thread forms its row's A x over the published column while
+//       reflector j is derived from the four partials (summed in one order:
+//       the same scalars everywhere); the column stands for u except at its
+//       first element, u0 instead of x0, which the row's element A[r][j+1]
+//       (= A[j+1][r], read from the published row) corrects in
+//       p = tau A u; then p, u and a partial of u'p are published;
+//   (c) K = tau/2 u'p, w_c = p_c - K u_c and the rank-2 update
+//       A -= u w' + w u' of the thread's nine elements.
+// The published vectors are zero outside the active rows, so no element
+// needs a mask, and the finished part of the register matrix no longer
+// changes.  Same outputs as eig_tridiag.
+__device__ __forceinline__ void eig_tridiag_reg(double* A, int lda, int n, const EigVecs& V) {
+  __shared__ __align__(16) double s_x[40];
+  __shared__ __align__(16) double s_row[40];
+  __shared__ __align__(16) double s_u[40];
+  __shared__ __align__(16) double s_p[40];
+  __shared__ __align__(16) double s_part[4];
+  __shared__ __align__(16) double s_kp[4];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int q = t & 3, r = (t >> 2) + 1, rowl = lane & ~3;
   const bool live = r < n;
-  double a[NC];
+  const int pr = qpos(r);
+  double a[9];
 #pragma unroll
-  for (int c = 0; c < NC; ++c) a[c] = (live && c < n) ? A[r * lda + c] : 0.0;
-  if (lane == 0) {
-    V.d[0] = A[0];
-    s_u[0] = s_u[NC] = 0.0;
-    s_w[0] = s_w[NC] = 0.0;
+  for (int i = 0; i < 9; ++i) {
+    const int c = 9 * q + i;
+    a[i] = (live && c < n) ? A[r * lda + c] : 0.0;
   }
-  const double2* u2 = reinterpret_cast<const double2*>(s_u);
-  const double2* w2 = reinterpret_cast<const double2*>(s_w);
+  if (t < 8) {  // entries that no row writes: column 0, quarter padding, columns 33..35
+    const int z = t == 0 ? 0 : (t < 4 ? 10 * t - 1 : 32 + t);
+    s_x[z] = s_row[z] = s_u[z] = s_p[z] = 0.0;
+  }
+  if (t == 0) V.d[0] = A[0];
+  const double2* x2 = reinterpret_cast<const double2*>(s_x + 10 * q);
+  const double2* u2 = reinterpret_cast<const double2*>(s_u + 10 * q);
+  const double2* p2 = reinterpret_cast<const double2*>(s_p + 10 * q);
+  double2* row2 = reinterpret_cast<double2*>(s_row + 10 * q);
+  int jq = 0, jr = 0;  // j = 9 jq + jr
+  int pj1 = 1;         // qpos(j + 1)
   for (int j = 0; j + 2 < n; ++j) {
-    const double x = reg_pick33(a, j);  // A[r][j]
-    if (j >= 1 && lane == j - 1) V.d[j] = x;  // row j is final after step j-1
-    const double s = warp_sum((live && r >= j + 2) ? x * x : 0.0);
-    const double x0 = __shfl_sync(~0u, x, j);  // A[j+1][j]
+    // (a)
+    const double x = __shfl_sync(~0u, reg_pick9(a, jr), rowl | jq);  // A[r][j]
+    const bool act = r >= j + 1;
+    const double xp = act ? x : 0.0;
+    if (q == 0) {
+      if (r == j) V.d[j] = x;  // row j is final after step j-1
+      s_x[pr] = xp;
+    }
+    if (r == j + 1) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) row2[i] = make_double2(a[2 * i], a[2 * i + 1]);
+      s_row[10 * q + 8] = a[8];
+    }
+    double sq = (q == 0 && r >= j + 2) ? x * x : 0.0;
+    sq += __shfl_xor_sync(~0u, sq, 4);
+    sq += __shfl_xor_sync(~0u, sq, 8);
+    sq += __shfl_xor_sync(~0u, sq, 16);
+    if (lane == 0) s_part[wid] = sq;
+    bar_named(1, 128);
+    // (b)
+    const double x0 = s_x[pj1];
+    double pp0 = 0.0, pp1 = 0.0;  // A x over the published column, before the reflector is known
+#pragma unroll
+    for (int i2 = 0; i2 < 5; ++i2) {
+      const double2 v = x2[i2];
+      pp0 = fma(a[2 * i2], v.x, pp0);
+      if (i2 < 4) pp1 = fma(a[2 * i2 + 1], v.y, pp1);
+    }
+    double pp = pp0 + pp1;
+    pp += __shfl_xor_sync(~0u, pp, 1);
+    pp += __shfl_xor_sync(~0u, pp, 2);
     double u0, tau, e;
-    eig_reflector(x0, s, u0, tau, e);
-    const bool act = live && r >= j + 1;
-    const double ur = !act ? 0.0 : (r == j + 1 ? u0 : x);
-    s_u[r] = ur;
-    if (act) A[j * lda + r] = ur;
-    if (lane == 0) {
+    eig_reflector_nb(x0, (s_part[0] + s_part[1]) + (s_part[2] + s_part[3]), u0, tau, e);
+    const double aj1 = s_row[pr];  // A[j+1][r]
+    const double ur = (r == j + 1) ? u0 : xp;
+    const double p = act ? tau * fma(aj1, u0 - x0, pp) : 0.0;
+    double kp = q == 0 ? ur * p : 0.0;
+    kp += __shfl_xor_sync(~0u, kp, 4);
+    kp += __shfl_xor_sync(~0u, kp, 8);
+    kp += __shfl_xor_sync(~0u, kp, 16);
+    if (lane == 0) s_kp[wid] = kp;
+    if (q == 0) {
+      s_p[pr] = p;
+      s_u[pr] = ur;
+      if (act && live) A[j * lda + r] = ur;
+    }
+    if (t == 0) {
       V.e[j] = e;
       V.u0[j] = u0;
       V.tau[j] = tau;
     }
-    __syncwarp();
-    double pa[4] = {0.0, 0.0, 0.0, 0.0};
+    bar_named(1, 128);
+    // (c)
+    const double K = 0.5 * tau * ((s_kp[0] + s_kp[1]) + (s_kp[2] + s_kp[3]));
+    const double wr = fma(-K, ur, p);
 #pragma unroll
-    for (int c2 = 0; c2 <= NC / 2; ++c2) {
-      const double2 u = u2[c2];
-      pa[c2 & 3] = fma(a[2 * c2], u.x, pa[c2 & 3]);
-      if (2 * c2 + 1 < NC) pa[c2 & 3] = fma(a[2 * c2 + 1], u.y, pa[c2 & 3]);
+    for (int i2 = 0; i2 < 5; ++i2) {
+      const double2 u = u2[i2], pv = p2[i2];
+      {
+        const double wc = fma(-K, u.x, pv.x);
+        a[2 * i2] = fma(-ur, wc, fma(-wr, u.x, a[2 * i2]));
+      }
+      if (i2 < 4) {
+        const double wc = fma(-K, u.y, pv.y);
+        a[2 * i2 + 1] = fma(-ur, wc, fma(-wr, u.y, a[2 * i2 + 1]));
+      }
     }
-    const double p = tau * ((pa[0] + pa[1]) + (pa[2] + pa[3]));
-    const double K = 0.5 * tau * warp_sum(ur * p);
-    const double wr = act ? fma(-K, ur, p) : 0.0;
-    s_w[r] = wr;
-    __syncwarp();
-#pragma unroll
-    for (int c2 = 0; c2 <= NC / 2; ++c2) {
-      const double2 u = u2[c2], w = w2[c2];
-      a[2 * c2] = fma(-ur, w.x, fma(-wr, u.x, a[2 * c2]));
-      if (2 * c2 + 1 < NC) a[2 * c2 + 1] = fma(-ur, w.y, fma(-wr, u.y, a[2 * c2 + 1]));
+    if (++jr == 9) {
+      jr = 0;
+      ++jq;
     }
-    __syncwarp();  // s_u and s_w are rewritten by the next step
+    pj1 = qpos(j + 2);
   }
-  const double y = reg_pick33(a, n - 2);
-  const double z = reg_pick33(a, n - 1);
-  if (lane == n - 3) V.d[n - 2] = y;
-  if (lane == n - 2) {
-    V.e[n - 2] = y;  // A[n-1][n-2]
-    V.d[n - 1] = z;
+  // d_{n-2} = A[n-2][n-2], e_{n-2} = A[n-1][n-2], d_{n-1} = A[n-1][n-1].
+  const double y = reg_pick9(a, (n - 2) % 9);
+  const double z = reg_pick9(a, (n - 1) % 9);
+  if (q == (n - 2) / 9) {
+    if (r == n - 2) V.d[n - 2] = y;
+    if (r == n - 1) V.e[n - 2] = y;
   }
+  if (q == (n - 1) / 9 && r == n - 1) V.d[n - 1] = z;
 }
 
 // Rescales a pair of consecutive minors by a power of two when the newer one
@@ -478,7 +550,7 @@ __device__ __forceinline__ void eig_gram(double* A, int lda, int n, const EigVec
   }
 }
 
-// 3. Three steps of inverse iteration on T - sigma I from a fixed start
+// 3. kEigInverseSteps steps of inverse iteration on T - sigma I from a fixed start
 // vector; warp 0.  Writes V.y (scaled down whenever its largest element
 // passes 1e100).
 __device__ __forceinline__ void eig_inverse_iteration(int n, const EigVecs& V, double sigma) {
@@ -532,7 +604,7 @@ __device__ __forceinline__ void eig_inverse_iteration(int n, const EigVecs& V, d
   for (int i = lane; i < n; i += 32) l[i] = i > 0 ? e[i - 1] * ru[i - 1] : 0.0;
   __syncwarp();
   if (lane == 0) {
-    for (int it = 0; it < 3; ++it) {
+    for (int it = 0; it < kEigInverseSteps; ++it) {
       // L z = y: z_i = y_i - l_i z_{i-1}, in chunks of four (loads first).
       double prev = y[0];
       int i = 1;
@@ -595,8 +667,8 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
     __syncthreads();
     return;
   }
-  if (n >= 3 && n <= kEigWarpRows) {
-    if (warp == 0) eig_tridiag_warp(A, lda, n, V);
+  if (n >= 3 && n <= kEigRegRows) {
+    if (warp < 4) eig_tridiag_reg(A, lda, n, V);
   } else if (warp < eig_tridiag_warps(n)) {
     eig_tridiag(A, lda, n, V);
   }

@@ -135,8 +135,10 @@ constexpr int kLeaderSections = 16;
 
 // Phases of the column kernel timed into ColumnLaunch::sect (thread 0 of each
 // CTA, summed): 0 entry decode and integral value, 1 slot probe, 2 x load,
-// z atomic and score, 3 candidate offer, 4 rounds counted.
-constexpr int kColumnSections = 5;
+// z atomic and score, 3 candidate offer, 4 rounds counted, 5 prelude (CTA
+// start to the first round), 6 CTA list merge, store and ticket, 7 the
+// column's final merge (last CTA), 8 CTAs counted, 9 final merges counted.
+constexpr int kColumnSections = 10;
 
 // Launchers (column_kernel.cu / leader_kernel.cu).
 int column_entries(int norb, int na, int nb);

@@ -354,9 +354,8 @@ __device__ void finish_iteration(IterState* S, const TableDev& T) {
   if (static_cast<int>(threadIdx.x) < k) {
     Slot* sp = T.slots + S->slot[threadIdx.x];
     sp->z = S->newz[threadIdx.x];
-    __threadfence();
   }
-  __syncthreads();
+  __syncthreads();  // orders the stores for this CTA; the next launch sees them anyway
   if (threadIdx.x < 32) {
     dd acc{0.0, 0.0};
     for (int c = threadIdx.x; c < k; c += 32) acc = dd_add_d(acc, S->dot[c]);

@@ -5,8 +5,9 @@ kernel and of the column kernel, on a synthetic workload.
         [--max-memory 16] [--warmup 300] [--iterations 300]
 
 Prints, per iteration, the device time of the two kernels (CUDA events) and
-the SM cycles of each leader phase (one CTA) and, per round of 256 column
-entries, of each column-kernel phase (thread 0 of each CTA).
+the SM cycles of each leader phase (one CTA); per round of 256 column entries,
+of each column-kernel phase (thread 0 of each CTA); and per column-kernel CTA
+its prelude and list merge, with the column's final merge by its last CTA.
 """
 import argparse
 import json
@@ -42,12 +43,18 @@ def main():
         lead = s.leader_sections()
         col = s.column_sections(enable=False)
         rounds = max(col.pop("rounds"), 1)
+        ctas = max(col.pop("ctas"), 1)
+        merges = max(col.pop("merges"), 1)
+        per_cta = {"prelude": round(col.pop("prelude") / ctas), "post": round(col.pop("post") / ctas),
+                   "merge": round(col.pop("merge") / merges)}
         print(json.dumps({
             "workload": args.workload, "k": args.k, "iterations": n,
             "leader_us_per_iteration": 1000.0 * t["leader_ms"] / n,
             "column_us_per_iteration": 1000.0 * t["column_ms"] / n,
             "leader_cycles_per_iteration": {k: round(v / n) for k, v in lead.items()},
             "column_cycles_per_round": {k: round(v / rounds) for k, v in col.items()},
+            "column_cycles_per_cta": per_cta,
+            "column_rounds_per_cta": round(rounds / ctas, 2),
         }, indent=1))
 
 

@@ -386,17 +386,14 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
       u2 += w_upd[w];
       i2 += w_ins[w];
     }
-    L.part_sum[2 * part] = nz;
-    L.part_sum[2 * part + 1] = dt;
-    if (e2) {
-      atomicAdd(&S->emitted, e2);
-      atomicAdd(&S->emitted_total, e2);
-    }
-    if (u2) {
-      atomicAdd(&S->updates, u2);
-      atomicAdd(&S->updates_total, u2);
-    }
-    if (i2) atomicAdd(&S->z_size, i2);
+    // The counters travel with the sums (exact in a double) and are added
+    // once per column by its last CTA, not by every CTA into the same words.
+    double* ps = L.part_sum + kPartSum * part;
+    ps[0] = nz;
+    ps[1] = dt;
+    ps[2] = static_cast<double>(e2);
+    ps[3] = static_cast<double>(u2);
+    ps[4] = static_cast<double>(i2);
   }
   __threadfence();
   __syncthreads();
@@ -428,13 +425,33 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
     }
     // Column sums in a fixed order: lane-strided partials, then a fixed tree.
     double nz = 0.0, dt = 0.0;
+    unsigned long long ce = 0, cu = 0, ci = 0;
     for (int gg = lane; gg < G; gg += 32) {
-      nz += __ldcg(L.part_sum + 2 * (base + gg));
-      dt += __ldcg(L.part_sum + 2 * (base + gg) + 1);
+      const double* ps = L.part_sum + kPartSum * (base + gg);
+      nz += __ldcg(ps);
+      dt += __ldcg(ps + 1);
+      ce += static_cast<unsigned long long>(__ldcg(ps + 2));
+      cu += static_cast<unsigned long long>(__ldcg(ps + 3));
+      ci += static_cast<unsigned long long>(__ldcg(ps + 4));
     }
     nz = warp_sum(nz);
     dt = warp_sum(dt);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ce += __shfl_xor_sync(~0u, ce, o);
+      cu += __shfl_xor_sync(~0u, cu, o);
+      ci += __shfl_xor_sync(~0u, ci, o);
+    }
     if (lane == 0) {
+      if (ce) {
+        atomicAdd(&S->emitted, ce);
+        atomicAdd(&S->emitted_total, ce);
+      }
+      if (cu) {
+        atomicAdd(&S->updates, cu);
+        atomicAdd(&S->updates_total, cu);
+      }
+      if (ci) atomicAdd(&S->z_size, ci);
       S->newz[col] = nz;
       S->dot[col] = dt;
       S->cand_n[col] = n;

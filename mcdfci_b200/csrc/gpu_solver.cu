@@ -313,7 +313,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     const size_t parts = static_cast<size_t>(opt_.k) * groups_;
     d_part_key_ = device_alloc<unsigned long long>(parts * list_, "column partial lists");
     d_part_slot_ = device_alloc<unsigned>(parts * list_, "column partial lists");
-    d_part_sum_ = device_alloc<double>(parts * 2, "column partial sums");
+    d_part_sum_ = device_alloc<double>(parts * kPartSum, "column partial sums");
     d_done_ = device_alloc<unsigned>(kMaxK, "column tickets");
     check(cudaMemsetAsync(d_done_, 0, kMaxK * sizeof(unsigned), stream_), "memset");
   } catch (...) {

@@ -72,7 +72,7 @@ struct ColumnLaunch {
   unsigned* cand_slot;    // [kMaxK][m] their hash slots (tables have at most 2^32 slots)
   unsigned long long* part_key;  // [kMaxK][groups][list] per-CTA candidate lists
   unsigned* part_slot;           // [kMaxK][groups][list]
-  double* part_sum;              // [kMaxK][groups][2] per-CTA new_z and dot partial sums
+  double* part_sum;              // [kMaxK][groups][kPartSum] per-CTA new_z, dot and entry counters
   unsigned* done;                // [kMaxK] CTAs finished per column (reset by the last one)
   unsigned long long* sect;  // [kColumnSections] SM cycles per phase of thread 0's rounds, or null
   int m;
@@ -100,6 +100,10 @@ struct LeaderLaunch {
 // every CTA reads its instance's descriptor from the constant bank.  All
 // instances of a batch share k and m.
 constexpr int kMaxBatch = 64;
+
+// Per-CTA partial values of the column kernel: new_z, dot, and the emitted,
+// updated and inserted entry counts (exact in a double).
+constexpr int kPartSum = 5;
 struct LeaderBatch {
   int n;
   LeaderLaunch L[kMaxBatch];

@@ -91,6 +91,28 @@ def test_incremental_scalars_match_table(fcidumps):
         assert abs(xz - txz) <= 1e-10 * abs(xz)
 
 
+def test_column_counters_match_oracle(fcidumps):
+    """The per-iteration counters of the report: |H[I]|_0 (cols_size, the
+    reference's sum of column lengths, src/solver.h:764-766) equals the
+    oracle's column lengths of the picked determinants, and with z_threshold
+    = 0 every entry is found or inserted (updates == cols_size)."""
+    path = fcidumps["h2o_sto3g"]
+    o = Oracle(path, 0.0)
+    s = m.CDFCI(m.Fcidump(path), threshold=0.0, max_memory=0.005, num_of_coordinate=8, estimate=8,
+                z_threshold=0.0)
+    s.reset()
+    total = 0
+    for it in range(4):
+        s.run_iterations(1)
+        r = s.report()
+        a, b, _ = s.picked()
+        want = sum(len(o.column_ab(int(x), int(y))[0]) for x, y in zip(a, b))
+        assert r["cols_size"] == want, (it, r["cols_size"], want)
+        assert r["updates"] == want
+        total += want
+    assert r["emitted_total"] - total == len(o.column(o.hartree_fock())[0])  # plus the initial column
+
+
 def test_overflow_is_reported_not_hung(synth_fcidumps):
     s = m.CDFCI(m.Fcidump(synth_fcidumps["n24_6a6b"]), threshold=0.0, max_memory=1e-4, num_of_coordinate=8,
                 estimate=8, num_iterations=50, report_interval=10)

@@ -275,15 +275,15 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool timed = L.sect != nullptr && threadIdx.x == 0;
   const long long c_start = timed ? clock64() : 0;
-  if (warp == 0) build_prelude(P, S->det[col], L.ham.norb);
-  __syncthreads();
-
+  // The column's scalars are read while warp 0 decodes the determinant.
   const double dxc = S->dx[col];
   const double hd = S->hdiag[col];
   const dd xss = S->xss;
   const dd scale = S->scale;
   const dd zt{S->zt, 0.0};
   const unsigned dslot = static_cast<unsigned>(S->slot[col]);
+  if (warp == 0) build_prelude(P, S->det[col], L.ham.norb);
+  __syncthreads();
   const int total = P.total;
   const int per = (total + G - 1) / G;
   const int beg = min(total, g * per);
@@ -395,7 +395,9 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
     ps[3] = static_cast<double>(u2);
     ps[4] = static_cast<double>(i2);
   }
-  __threadfence();
+  // Only warp 0 wrote what the column's last CTA reads (the list and the
+  // partial sums); its fence orders those writes before the ticket.
+  if (warp == 0) __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) s_last = (atomicAdd(L.done + col, 1u) == static_cast<unsigned>(G - 1));
   __syncthreads();

@@ -478,7 +478,11 @@ void GpuSolver::read_state() {
   if (err) {
     if (err & (kErrProbe | kErrOverflow))
       throw McdError(MCD_ERR_OVERFLOW, "The hash table is full. Please increase max_memory or z_threshold.");
-    if (err & kErrEig) throw McdError(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
+    if (err & kErrEig)
+      throw McdError(MCD_ERR_EIG,
+                     "The subspace eigenvalue problem failed (its lowest eigenvalue must be negative: the method "
+                     "minimises ||H + x x^T||_F^2, which needs a negative ground-state energy; a positive core "
+                     "energy in the FCIDUMP can make it positive).");
     if (err & kErrCandidates) throw McdError(MCD_ERR_NO_CANDIDATES, "The candidate list is empty.");
     throw McdError(MCD_ERR_CUDA, "device error word " + std::to_string(err));
   }

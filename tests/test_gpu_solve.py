@@ -113,6 +113,37 @@ def test_column_counters_match_oracle(fcidumps):
     assert r["emitted_total"] - total == len(o.column(o.hartree_fock())[0])  # plus the initial column
 
 
+@pytest.mark.parametrize("norb,na,nb", [(2, 1, 1), (3, 1, 1), (4, 2, 1)])
+def test_space_smaller_than_k(norb, na, nb, tmp_path):
+    """Determinant spaces of 4, 9 and 24 states with k = m = 8: the candidate
+    lists hold fewer distinct determinants than k, so every iteration picks
+    all it has (k = min(candidates, num_of_coordinate)); the solve still
+    reaches the dense FP64 ground state.  The integrals keep the ground-state
+    energy negative, which the method requires (it minimises
+    ||H + x x^T||_F^2)."""
+    from itertools import combinations
+
+    from mcdfci_b200 import synth
+
+    path = str(tmp_path / "small.fcidump")
+    synth.write_fcidump(path, synth.SynthSpec(norb, na, nb, -20.0, -10.0, 0.1, 2 * norb, ecore=-5.0), seed=1)
+    o = Oracle(path, 0.0)
+    dets = [(sum(1 << p for p in a), sum(1 << p for p in b)) for a in combinations(range(norb), na)
+            for b in combinations(range(norb), nb)]
+    idx = {d: i for i, d in enumerate(dets)}
+    H = np.zeros((len(dets), len(dets)))
+    for d in dets:
+        cd, cv = o.column_ab(*d)
+        for e, v in zip(cd, cv):
+            H[idx[e], idx[d]] = v
+    e0 = np.linalg.eigvalsh(H)[0]
+    assert e0 < 0.0
+    s, e = _solve(path, num_iterations=2000, report_interval=500, max_memory=0.001, num_of_coordinate=8,
+                  estimate=8)
+    assert abs(e - e0) < 1e-8, (e, e0)
+    assert s.reports[-1]["last_k"] <= len(dets)
+
+
 def test_overflow_is_reported_not_hung(synth_fcidumps):
     s = m.CDFCI(m.Fcidump(synth_fcidumps["n24_6a6b"]), threshold=0.0, max_memory=1e-4, num_of_coordinate=8,
                 estimate=8, num_iterations=50, report_interval=10)

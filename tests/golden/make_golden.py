@@ -19,6 +19,7 @@ from its sources).  Outputs:
   hsub_*.json.gz              get_hamiltonian_submatrix output for random det sets
   eig_*.json.gz               CoordinateUpdateEig inputs/outputs captured in real runs
   energies.json               converged energies printed by the reference solver
+  trajectories.json           report energies of small-k solves (--only trajectories)
 
 Determinants in these files use the reference layout: interleaved spin-orbital
 bits (bit 2p = alpha p, bit 2p+1 = beta p) in 64-bit words, word 0 first.
@@ -79,6 +80,30 @@ def final_energy(stdout: str) -> float:
     return float(rows[-1].split()[1])
 
 
+def report_energies(stdout: str):
+    rows = [l for l in stdout.splitlines() if re.match(r"^\d+\s+-?\d+\.\d+", l)]
+    return [[int(l.split()[0]), float(l.split()[1])] for l in rows]
+
+
+def trajectories() -> None:
+    """trajectories.json: the reference's report energies (every 250
+    iterations) on the 7-orbital fixture for k = 1 (m = 1) and k = 2 (m = 4)."""
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        n7 = os.path.join(tmp, "n7.fcidump")
+        gunzip_to(os.path.join(HERE, "n7_5a5b.fcidump.gz"), n7)
+        for k, m in ((1, 1), (2, 4)):
+            j = os.path.join(tmp, "n7_k%d.json" % k)
+            write_input(j, n7, num_iterations=2000, report_interval=250, z_threshold=0,
+                        z_threshold_search=False, max_memory=0.001, coordinate_pick="gcd_grad",
+                        coordinate_update="eig", num_of_coordinate=k, estimate=m)
+            out["n7_5a5b k%d m%d" % (k, m)] = report_energies(run([CDFCI, j]))
+    with open(os.path.join(HERE, "trajectories.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+        f.write("\n")
+    print(json.dumps(out, indent=1))
+
+
 def write_input(path, fcidump, **kw):
     synth.write_input_json(path, fcidump, **kw)
 
@@ -86,7 +111,10 @@ def write_input(path, fcidump, **kw):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", choices=["all", "trajectories"], default="all")
     args = ap.parse_args()
+    if args.only == "trajectories":
+        return trajectories()
     for exe in (REF_DUMP, CDFCI):
         if not os.path.exists(exe):
             sys.exit(f"missing {exe}: run `make -C oracle ref` first")

@@ -180,3 +180,24 @@ def test_cli_error_exit(tmp_path):
     deck.write_text('{"hamiltonian": {"fcidump_path": "/nonexistent"}, "solver": {"cdfci": {"max_memory": 1}}}')
     res = subprocess.run([m.CLI_PATH, str(deck)], capture_output=True, text=True, timeout=60)
     assert res.returncode == 1 and "ERROR:" in res.stderr
+
+
+TRAJECTORIES = load_golden("trajectories.json")
+
+
+@pytest.mark.parametrize("k,mm,upto", [(1, 1, 2000), (2, 4, 1000)])
+def test_small_k_trajectory_matches_reference(k, mm, upto, fcidumps):
+    """Energies at every report (each 250 iterations) of k = 1 and k = 2
+    solves on the 7-orbital fixture against the reference's own run
+    (tests/golden/trajectories.json).  With one or two columns per iteration
+    the picks follow the same rule on both sides, so the trajectories agree
+    report by report; alpha/beta mirror choices give equal energies.  The
+    reference's k = 2 run is compared up to iteration 1000: beyond that its
+    own runs differ from one another at 1e-8."""
+    want = [e for it, e in TRAJECTORIES["n7_5a5b k%d m%d" % (k, mm)] if it <= upto]
+    s, _ = _solve(fcidumps["n7_5a5b"], num_iterations=upto, report_interval=250, max_memory=0.001,
+                  num_of_coordinate=k, estimate=mm, z_threshold=0.0)
+    got = [r["energy"] for r in s.reports]
+    assert len(got) == len(want)
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert abs(g - w) < 1e-8, (250 * (i + 1), g, w)

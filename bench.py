@@ -391,6 +391,11 @@ def b200_arm(args, rank, world, local_rank):
         col_ms_avg = t["column_ms"] / args.steps
         total_max = max_over_ranks(total_s, dist, "cuda")
         value = replica_rate(updates, total_s, world, dist, "cuda")
+        # The scattered-access ceiling of the same table: as many pseudo-random
+        # slots as a launch has entries, each touched the way an entry touches
+        # its slot (key, x, atomic z add of zero), 1 or 4 in flight per thread.
+        per_launch = max(1, int(entries / args.steps))
+        scatter = max(solver.scatter_rate(per_launch, 20, 1), solver.scatter_rate(per_launch, 20, 4))
         solver.close()
 
         peak, peak_kind = hbm_peak()
@@ -400,7 +405,12 @@ def b200_arm(args, rank, world, local_rank):
                     "traffic": traffic, "peak_source": peak_kind,
                     "kernel": "column_kernel", "entries_per_launch": entries / args.steps,
                     "algorithmic_bytes_per_entry": BYTES_PER_ENTRY, "avg_launch_ms": col_ms_avg,
-                    "leader_ms_per_step": t["leader_ms"] / args.steps}
+                    "leader_ms_per_step": t["leader_ms"] / args.steps,
+                    "scatter_ceiling": {"slots_per_s": scatter,
+                                        "column_entries_per_s": (entries / args.steps) / (col_ms_avg / 1000.0),
+                                        "frac": (entries / args.steps) / (col_ms_avg / 1000.0) / scatter,
+                                        "probe": "mcd_debug_scatter_rate on the same table, best of 1 and 4 "
+                                                 "slots in flight per thread, 148 x 8 CTAs of 256"}}
 
         e2e = None
         if not args.no_e2e:

@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
     "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_launch_info", "mcd_debug_leader_sections",
+    "mcd_debug_scatter_rate",
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
@@ -156,6 +157,7 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
     L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
+    L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _dp]
     L.mcd_debug_leader_sections.argtypes = [vp, _u64p, ctypes.c_int32]
     _lib = L
     return L
@@ -476,6 +478,13 @@ class CDFCI:
         v = np.zeros(16, dtype=np.uint64)
         _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), 16))
         return {name: int(c) for name, c in zip(self.LEADER_SECTIONS, v)}
+
+    def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1) -> float:
+        """Slots per second of the table's scattered-access probe (a column
+        entry's key read, x read and atomic z add, at pseudo-random slots)."""
+        r = ctypes.c_double()
+        _check(library().mcd_debug_scatter_rate(self._h, int(entries), int(reps), int(ilp), ctypes.byref(r)))
+        return r.value
 
     def launch_info(self) -> dict:
         c, mac, e = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

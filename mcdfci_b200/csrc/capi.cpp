@@ -616,6 +616,14 @@ int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_
   });
 }
 
+int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, double* slots_per_s) {
+  return guarded([&] {
+    if (!s || !slots_per_s) return fail(MCD_ERR_INVALID, "NULL argument.");
+    *slots_per_s = s->impl->scatter_rate(entries, reps, ilp);
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, int32_t* entries) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");

@@ -756,6 +756,45 @@ cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Scattered-access ceiling of the table, for the column kernel's roofline: a
+// stream of pseudo-random slots, each touched the way a column entry touches
+// its slot (the 16-byte key, then x and an FP64 atomic add on z that returns
+// the old value; the add is of zero, so the table keeps its values).  ILP
+// slots are in flight per thread; the grid fills every SM.
+template <int ILP>
+__global__ void __launch_bounds__(256) scatter_probe_kernel(Slot* slots, uint64_t mask, long long entries,
+                                                            uint64_t seed, double* sink) {
+  double acc = 0.0;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x * ILP;
+  for (long long e0 = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) * ILP; e0 < entries;
+       e0 += stride) {
+    uint64_t sl[ILP], ka[ILP], kb[ILP];
+#pragma unroll
+    for (int q = 0; q < ILP; ++q) {
+      sl[q] = fmix64(seed ^ static_cast<uint64_t>(e0 + q)) & mask;
+      if (e0 + q < entries) load_key(slots + sl[q], ka[q], kb[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < ILP; ++q) {
+      if (e0 + q < entries && ka[q] != ~0ull - 1ull) {  // uses the key, as a probe does
+        Slot* sp = slots + sl[q];
+        acc += sp->x + atomicAdd(&sp->z, 0.0) + static_cast<double>(kb[q] & 1ull);
+      }
+    }
+  }
+  if (acc == 1234.5678) *sink = acc;  // keeps the loads
+}
+
+cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, uint64_t seed, double* sink,
+                          cudaStream_t s) {
+  const int ctas = 148 * 8;
+  if (ilp >= 4)
+    scatter_probe_kernel<4><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
+  else
+    scatter_probe_kernel<1><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
+  return cudaGetLastError();
+}
+
 cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,
                          double* v_out, int cap, int* n_out, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(n_out, 0, sizeof(int), s);

@@ -1013,6 +1013,33 @@ std::vector<unsigned long long> GpuSolver::column_sections(bool enable) {
   return v;
 }
 
+double GpuSolver::scatter_rate(long long entries, int reps, int ilp) {
+  if (entries <= 0 || reps <= 0) throw McdError(MCD_ERR_INVALID, "entries and reps must be positive.");
+  double* sink = device_alloc<double>(1, "probe");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float ms = 0.0f;
+  try {
+    check(cudaEventCreate(&e0), "cudaEventCreate");
+    check(cudaEventCreate(&e1), "cudaEventCreate");
+    check(scatter_probe(td_, entries, ilp, 0x5eedull, sink, stream_), "scatter probe");
+    check(cudaEventRecord(e0, stream_), "cudaEventRecord");
+    for (int r = 0; r < reps; ++r)
+      check(scatter_probe(td_, entries, ilp, 0x5eedull + 7919ull * (r + 1), sink, stream_), "scatter probe");
+    check(cudaEventRecord(e1, stream_), "cudaEventRecord");
+    check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(sink);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  return static_cast<double>(entries) * reps / (static_cast<double>(ms) * 1e-3);
+}
+
 std::vector<unsigned long long> GpuSolver::leader_sections() {
   std::vector<unsigned long long> v(kLeaderSections);
   check(cudaStreamSynchronize(stream_), "sync");

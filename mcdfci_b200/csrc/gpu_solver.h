@@ -90,6 +90,9 @@ class GpuSolver {
   // Column-kernel phase timers (kColumnSections values since the last call,
   // which resets them); `enable` turns them on or off for later launches.
   std::vector<unsigned long long> column_sections(bool enable);
+  // Slots per second of the scattered-access probe on this solver's table
+  // (reps timed launches of `entries` slots after one untimed launch).
+  double scatter_rate(long long entries, int reps, int ilp);
 
   const HamHost& ham() const { return ham_; }
   Det reference_det() const { return ref_; }

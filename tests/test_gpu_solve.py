@@ -144,6 +144,24 @@ def test_space_smaller_than_k(norb, na, nb, tmp_path):
     assert s.reports[-1]["last_k"] <= len(dets)
 
 
+def test_scatter_probe_keeps_the_table(fcidumps):
+    """The scattered-access probe behind the column kernel's roofline runs on
+    the solver's table and leaves its values as they were (its z adds are of
+    zero)."""
+    s = m.CDFCI(m.Fcidump(fcidumps["h2o_sto3g"]), threshold=0.0, max_memory=0.005, num_of_coordinate=8,
+                estimate=8)
+    s.reset()
+    s.run_iterations(200)
+    before = s.table_sums()
+    for ilp in (1, 4):
+        assert s.scatter_rate(50_000, 3, ilp) > 0.0
+    after = s.table_sums()
+    assert after["occupied"] == before["occupied"]
+    for key in ("xx", "xz"):
+        b, a = sum(before[key]), sum(after[key])
+        assert abs(a - b) <= 1e-14 * abs(b), (key, a, b)
+
+
 def test_overflow_is_reported_not_hung(synth_fcidumps):
     s = m.CDFCI(m.Fcidump(synth_fcidumps["n24_6a6b"]), threshold=0.0, max_memory=1e-4, num_of_coordinate=8,
                 estimate=8, num_iterations=50, report_interval=10)

@@ -9,7 +9,10 @@ their 32 Hamiltonian columns (16,471 entries each), solve the 33x33 subspace
 eigenproblem, apply x += dx and z += H_col * dx in the hash wavefunction.
 
   value        coordinate updates/s over all ranks (32 per step per rank),
-               from CUDA events on the solver's stream, max over ranks
+               from CUDA events on the solver's stream around the product
+               path (CUDA graphs of 64 iterations), max over ranks; a pass of
+               direct launches with an event between the two kernels of every
+               iteration gives the per-kernel times of the roofline
   e2e          the same metric through the C ABI a user calls
                (mcd_create_from_fcidump from host data + mcd_solve + read of
                the result), wall clock, host<->device copies inside
@@ -378,15 +381,30 @@ def b200_arm(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank)
         sampler.start()
         time.sleep(0.3)
+        # Per-kernel device times (direct launches with an event between the
+        # two kernels of every iteration), for the roofline.
         t = solver.run_iterations_timed(args.steps)
+        r_mid = solver.report()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        # The timed steps: the product path, CUDA graphs of 64 iterations on
+        # the solver's stream, bracketed by events on that stream.
+        ext = torch.cuda.ExternalStream(solver.stream)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(ext)
+        solver.run_iterations(args.steps)
+        ev1.record(ext)
+        ev1.synchronize()
         torch.cuda.synchronize()
         sampler.stop()
         if dist:
             dist.barrier()
         r1 = solver.report()
         clocks = sampler.summary()
-        total_s = t["total_ms"] / 1000.0
-        entries = r1["emitted_total"] - r0["emitted_total"]
+        total_s = ev0.elapsed_time(ev1) / 1000.0
+        entries = r_mid["emitted_total"] - r0["emitted_total"]
         updates = args.k * args.steps
         col_ms_avg = t["column_ms"] / args.steps
         total_max = max_over_ranks(total_s, dist, "cuda")

@@ -40,6 +40,8 @@
 // (atomic ticket) merges them and writes the column's m candidates, new z and
 // dot products (summed in a fixed order).
 #include "device_common.cuh"
+#include <algorithm>
+
 #include "kernels.h"
 #include "toplist.cuh"
 
@@ -527,7 +529,7 @@ __global__ void rdm_list_kernel(const Slot* slots, size_t n, unsigned* list, uns
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const Slot sl = slots[i];
-    if (sl.a == kEmptyKey && sl.b == kEmptyKey) continue;
+    if (slot_vacant(sl.a, sl.b)) continue;
     if (sl.x == 0.0) continue;
     const unsigned long long j = atomicAdd(count, 1ull);
     if (j < cap) list[j] = static_cast<unsigned>(i);
@@ -717,10 +719,16 @@ int column_entries(int norb, int na, int nb) {
 
 int column_list_size(int m) { return m <= 32 ? 32 : (m <= 64 ? 64 : 128); }
 
-int column_groups(int entries, int k) {
-  (void)k;
-  // About three rounds of kNT entries per CTA.
-  const int g = (entries + 3 * kNT - 1) / (3 * kNT);
+int column_groups(int entries, int k, int resident) {
+  // About three rounds of kNT entries per CTA ...
+  int g = (entries + 3 * kNT - 1) / (3 * kNT);
+  // ... or, when k columns of such CTAs leave resident CTA slots empty, as
+  // many CTAs as fill them, down to one round each.
+  if (resident > 0 && k > 0) {
+    const int fill = (resident + k - 1) / k;
+    const int one_round = (entries + kNT - 1) / kNT;
+    g = std::max(g, std::min(fill, one_round));
+  }
   return g < 1 ? 1 : g;
 }
 

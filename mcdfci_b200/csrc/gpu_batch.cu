@@ -54,6 +54,7 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       SolverOptions each = opt_;
       each.stream = G.stream;
       each.verbose = false;
+      each.fill_gpu = false;  // the batch's columns fill the GPU together
       inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
       const int j = G.lb->n;
       G.lb->L[j] = inst_.back()->leader_launch();

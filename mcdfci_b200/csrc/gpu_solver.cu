@@ -19,9 +19,11 @@ namespace mcd {
 
 __global__ void table_fill_kernel(Slot* slots, size_t n) {
   const Slot e{kEmptyKey, kEmptyKey, 0.0, 0.0};
+  const Slot r{kEmptyKey, kReservedKeyB, 0.0, 0.0};
+  const bool reserve = n == (static_cast<size_t>(1) << 32);  // slot 2^32-1 is the "no slot" marker
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
-    slots[i] = e;
+    slots[i] = (reserve && i == n - 1) ? r : e;
 }
 
 __global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsigned long long* count) {
@@ -31,7 +33,7 @@ __global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsi
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const Slot s = slots[i];
-    if (s.a == kEmptyKey && s.b == kEmptyKey) continue;
+    if (slot_vacant(s.a, s.b)) continue;
     ++c;
     axx = dd_add(axx, dd_two_prod(s.x, s.x));
     axz = dd_add(axz, dd_two_prod(s.x, s.z));
@@ -64,7 +66,7 @@ __global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsi
 // again.  The current candidate lists are saved before and re-found after.
 
 __device__ __forceinline__ bool compact_keeps(const Slot& s, double zlim) {
-  if (s.a == kEmptyKey && s.b == kEmptyKey) return false;
+  if (slot_vacant(s.a, s.b)) return false;
   return s.x != 0.0 || fabs(s.z) > zlim;
 }
 
@@ -229,6 +231,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ref_diag_ = diagonal_element(ham_, ref_);
   na_ = __builtin_popcountll(ref_.a);
   nb_ = __builtin_popcountll(ref_.b);
+  if (na_ >= 64)  // its only determinant would carry the empty-slot key
+    throw McdError(MCD_ERR_UNSUPPORTED, "64 alpha electrons in 64 orbitals (a single determinant) is not supported.");
   entries_ = column_entries(ham_.norb, na_, nb_);
   if (entries_ < 0) throw McdError(MCD_ERR_UNSUPPORTED, "a Hamiltonian column has more than 2^31 entries.");
   n_words_ = 1 + (fci.norb - 1) / 64;
@@ -254,7 +258,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     own_stream_ = true;
   }
-  groups_ = opt_.groups > 0 ? opt_.groups : column_groups(entries_, opt_.k);
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "cudaDeviceGetAttribute");
+  groups_ = opt_.groups > 0 ? opt_.groups : column_groups(entries_, opt_.k, opt_.fill_gpu ? 3 * sms : 0);
   list_ = column_list_size(opt_.m);
 
   try {

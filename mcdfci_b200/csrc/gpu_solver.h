@@ -28,6 +28,7 @@ struct SolverOptions {
   int coordinate_pick = MCD_PICK_GCD_GRAD;
   int coordinate_update = MCD_UPDATE_EIG;
   int groups = 0;
+  bool fill_gpu = true;  // with groups = 0: spread few columns over more CTAs (a batch fills the GPU itself)
   bool compaction = false;
   bool verbose = false;
   cudaStream_t stream = nullptr;

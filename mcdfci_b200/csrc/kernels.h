@@ -149,7 +149,10 @@ int column_entries(int norb, int na, int nb);
 // Length of the per-CTA candidate lists for `estimate` m (32, 64 or 128).
 int column_list_size(int m);
 // CTAs per column for a column of `entries` entries.
-int column_groups(int entries, int k);
+// CTAs per column: about three rounds of 256 entries each, or more when k
+// such columns would leave some of `resident` CTA slots of the GPU empty
+// (resident = 0: never more).
+int column_groups(int entries, int k, int resident);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
 cudaError_t launch_leader_batch(const LeaderBatch& b, cudaStream_t s);

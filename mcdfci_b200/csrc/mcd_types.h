@@ -24,6 +24,14 @@ constexpr int kMaxM = 128;
 // Key of an empty hash slot.  A determinant can only equal it if all 64
 // alpha and all 64 beta orbitals are occupied.
 constexpr uint64_t kEmptyKey = ~0ull;
+// A table of exactly 2^32 slots keeps its last slot, whose index equals the
+// 32-bit "no slot" marker of the candidate lists, out of use: it holds the
+// key (kEmptyKey, kReservedKeyB), which no determinant of fewer than 64
+// alpha electrons matches, so every probe passes over it.
+constexpr uint64_t kReservedKeyB = ~0ull - 1ull;
+
+// A slot that holds no determinant: empty, or the reserved last slot.
+MCD_HD bool slot_vacant(uint64_t a, uint64_t b) { return a == kEmptyKey && (b == kEmptyKey || b == kReservedKeyB); }
 
 // A Slater determinant as a pair of occupation strings: bit p of `a` is the
 // alpha spin-orbital of spatial orbital p, bit p of `b` the beta one.  The

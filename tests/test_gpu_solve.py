@@ -219,3 +219,27 @@ def test_small_k_trajectory_matches_reference(k, mm, upto, fcidumps):
     assert len(got) == len(want)
     for i, (g, w) in enumerate(zip(got, want)):
         assert abs(g - w) < 1e-8, (250 * (i + 1), g, w)
+
+
+def test_table_of_2_32_slots_keeps_its_marker_slot_free(fcidumps):
+    """A max_memory that sizes the table to 2^32 slots (137 GB): the last slot,
+    whose index is the candidate lists' 32-bit "no slot" marker, is reserved
+    at every fill, so no determinant lands there and the table scans do not
+    count it; the solve reaches the reference's energy."""
+    import gc
+
+    import torch
+
+    gc.collect()
+    if torch.cuda.get_device_properties(0).total_memory < 150 * 2**30:
+        pytest.skip("needs a GPU with 150 GB")
+    big = m.CDFCI(m.Fcidump(fcidumps["h2o_sto3g"]), max_memory=140.0, threshold=0.0, num_of_coordinate=8,
+                  estimate=8)
+    try:
+        big.reset()
+        big.run_iterations(20000)
+        r = big.report()
+        assert abs(r["energy"] - ENERGIES["h2o_sto3g k8 m8 20000it"]) < 1e-6
+        assert big.table_sums()["occupied"] == r["occupied"]
+    finally:
+        big.close()

@@ -151,7 +151,7 @@ int column_list_size(int m);
 // CTAs per column for a column of `entries` entries.
 // CTAs per column: about three rounds of 256 entries each, or more when k
 // such columns would leave some of `resident` CTA slots of the GPU empty
-// (resident = 0: never more).
+// (resident = 0: never more); at most 96.
 int column_groups(int entries, int k, int resident);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);

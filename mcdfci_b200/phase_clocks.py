@@ -1,8 +1,8 @@
 """Where the device time of an iteration goes: the phase timers of the leader
 kernel and of the column kernel, on a synthetic workload.
 
-    python -m mcdfci_b200.phase_clocks [--workload n24_6a6b] [--k 32]
-        [--max-memory 16] [--warmup 300] [--iterations 300]
+    python -m mcdfci_b200.phase_clocks [--workload n24_6a6b] [--k 32] [--m 32]
+        [--max-memory 16] [--warmup 300] [--iterations 300] [--groups 0]
 
 Prints, per iteration, the device time of the two kernels (CUDA events) and
 the SM cycles of each leader phase (one CTA); per round of 256 column entries,
@@ -27,12 +27,13 @@ def main():
     ap.add_argument("--z-threshold", type=float, default=1e-9)
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--iterations", type=int, default=300)
+    ap.add_argument("--groups", type=int, default=0, help="CTAs per column (0: the library's choice)")
     args = ap.parse_args()
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, args.workload + ".fcidump")
         synth.write_fcidump(path, args.workload, seed=0)
         s = m.CDFCI(m.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
-                    z_threshold=args.z_threshold, threshold=0.0)
+                    z_threshold=args.z_threshold, threshold=0.0, groups=args.groups)
         s.reset()
         s.run_iterations(args.warmup)
         s.report()
@@ -48,7 +49,7 @@ def main():
         per_cta = {"prelude": round(col.pop("prelude") / ctas), "post": round(col.pop("post") / ctas),
                    "merge": round(col.pop("merge") / merges)}
         print(json.dumps({
-            "workload": args.workload, "k": args.k, "iterations": n,
+            "workload": args.workload, "k": args.k, "iterations": n, "groups": s.launch_info()["groups"],
             "leader_us_per_iteration": 1000.0 * t["leader_ms"] / n,
             "column_us_per_iteration": 1000.0 * t["column_ms"] / n,
             "leader_cycles_per_iteration": {k: round(v / n) for k, v in lead.items()},

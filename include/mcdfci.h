@@ -267,8 +267,10 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
  * roofline: slots per second over reps launches of `entries` pseudo-random
  * slots, each touched as a column entry touches its slot (16-byte key, x, an
  * FP64 atomic add of zero on z, so the values stay), ilp = 1 or 4 slots in
- * flight per thread.  No counterpart in the reference. */
-int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, double* slots_per_s);
+ * flight per thread, ctas_per_sm CTAs of 256 threads per SM (1..8; 0 = 8).
+ * No counterpart in the reference. */
+int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
+                           double* slots_per_s);
 /* SM cycles spent in each phase of the leader kernel (16 phases: state load,
  * finish, candidate gather, top-k, tie sort, picked, H_sub, update_x, publish,
  * eig setup, tridiagonalisation, multisection, inverse iteration,

@@ -157,7 +157,7 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
     L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
-    L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _dp]
+    L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
     L.mcd_debug_leader_sections.argtypes = [vp, _u64p, ctypes.c_int32]
     _lib = L
     return L
@@ -479,11 +479,13 @@ class CDFCI:
         _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), 16))
         return {name: int(c) for name, c in zip(self.LEADER_SECTIONS, v)}
 
-    def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1) -> float:
+    def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1, ctas_per_sm: int = 0) -> float:
         """Slots per second of the table's scattered-access probe (a column
-        entry's key read, x read and atomic z add, at pseudo-random slots)."""
+        entry's key read, x read and atomic z add, at pseudo-random slots),
+        with ctas_per_sm CTAs of 256 threads per SM (0: 8)."""
         r = ctypes.c_double()
-        _check(library().mcd_debug_scatter_rate(self._h, int(entries), int(reps), int(ilp), ctypes.byref(r)))
+        _check(library().mcd_debug_scatter_rate(self._h, int(entries), int(reps), int(ilp), int(ctas_per_sm),
+                                                ctypes.byref(r)))
         return r.value
 
     def launch_info(self) -> dict:

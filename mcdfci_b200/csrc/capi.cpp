@@ -616,10 +616,11 @@ int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_
   });
 }
 
-int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, double* slots_per_s) {
+int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
+                           double* slots_per_s) {
   return guarded([&] {
     if (!s || !slots_per_s) return fail(MCD_ERR_INVALID, "NULL argument.");
-    *slots_per_s = s->impl->scatter_rate(entries, reps, ilp);
+    *slots_per_s = s->impl->scatter_rate(entries, reps, ilp, ctas_per_sm);
     return MCD_OK;
   });
 }

@@ -798,9 +798,9 @@ __global__ void __launch_bounds__(256) scatter_probe_kernel(Slot* slots, uint64_
   if (acc == 1234.5678) *sink = acc;  // keeps the loads
 }
 
-cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, uint64_t seed, double* sink,
+cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
                           cudaStream_t s) {
-  const int ctas = 148 * 8;
+  if (ctas < 1) return cudaErrorInvalidValue;
   if (ilp >= 4)
     scatter_probe_kernel<4><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
   else

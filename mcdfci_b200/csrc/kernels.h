@@ -176,8 +176,9 @@ cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s);
 // Column of one determinant: writes up to `cap` (a, b, value) entries.
 // Scattered-access probe of the table: `entries` pseudo-random slots, each
 // read (key, x) and given an atomic add of zero on z; ilp 1 or 4 slots in
-// flight per thread.  `sink`: one device double, written only to keep loads.
-cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, uint64_t seed, double* sink,
+// flight per thread; `ctas` CTAs of 256 threads.  `sink`: one device double,
+// written only to keep loads.
+cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
                           cudaStream_t s);
 cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,
                          double* v_out, int cap, int* n_out, cudaStream_t s);

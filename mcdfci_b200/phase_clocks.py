@@ -2,7 +2,7 @@
 kernel and of the column kernel, on a synthetic workload.
 
     python -m mcdfci_b200.phase_clocks [--workload n24_6a6b] [--k 32] [--m 32]
-        [--max-memory 16] [--warmup 300] [--iterations 300] [--groups 0]
+        [--max-memory 16] [--warmup 300] [--iterations 300] [--groups 0] [--scatter]
 
 Prints, per iteration, the device time of the two kernels (CUDA events) and
 the SM cycles of each leader phase (one CTA); per round of 256 column entries,
@@ -28,6 +28,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=300)
     ap.add_argument("--iterations", type=int, default=300)
     ap.add_argument("--groups", type=int, default=0, help="CTAs per column (0: the library's choice)")
+    ap.add_argument("--scatter", action="store_true",
+                    help="also sweep the table's scattered-access probe (slots per launch, CTAs per SM, "
+                         "slots in flight per thread)")
     args = ap.parse_args()
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, args.workload + ".fcidump")
@@ -48,6 +51,14 @@ def main():
         merges = max(col.pop("merges"), 1)
         per_cta = {"prelude": round(col.pop("prelude") / ctas), "post": round(col.pop("post") / ctas),
                    "merge": round(col.pop("merge") / merges)}
+        scatter = []
+        if args.scatter:
+            for entries in (527072, 2108288, 8433152, 33732608):
+                for cps in (3, 8):
+                    for ilp in (1, 4):
+                        r = s.scatter_rate(entries, 10, ilp, cps)
+                        scatter.append({"slots": entries, "ctas_per_sm": cps, "ilp": ilp, "slots_per_s": r,
+                                        "us_per_launch": entries / r * 1e6})
         print(json.dumps({
             "workload": args.workload, "k": args.k, "iterations": n, "groups": s.launch_info()["groups"],
             "leader_us_per_iteration": 1000.0 * t["leader_ms"] / n,
@@ -56,6 +67,7 @@ def main():
             "column_cycles_per_round": {k: round(v / rounds) for k, v in col.items()},
             "column_cycles_per_cta": per_cta,
             "column_rounds_per_cta": round(rounds / ctas, 2),
+            "scatter_probe": scatter,
         }, indent=1))
 
 

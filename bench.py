@@ -81,6 +81,12 @@ def parse_args():
     ap.add_argument("--curve-iterations", type=int, default=20000)
     ap.add_argument("--curve-report", type=int, default=1000)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-curve throughput object")
+    ap.add_argument("--phases", action="store_true",
+                    help="print where the device time of an iteration goes (leader and column phase timers) "
+                         "on --phase-workload instead of the bench line")
+    ap.add_argument("--phase-workload", default="n24_6a6b")
+    ap.add_argument("--scatter-sweep", action="store_true",
+                    help="with --phases: also sweep the table's scattered-access probe")
     return ap.parse_args()
 
 
@@ -278,6 +284,59 @@ def curve_arm(args, local_rank):
         print(json.dumps(out))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def phases_arm(args, local_rank):
+    """Per-iteration device time of the two kernels (CUDA events) and the SM
+    cycles of each leader phase (one CTA), of each column-kernel phase per
+    round of 256 entries (thread 0 of each CTA), and per column-kernel CTA its
+    prelude and list merge, with the column's final merge by its last CTA."""
+    import mcdfci_b200 as mc
+    from mcdfci_b200 import synth
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, args.phase_workload + ".fcidump")
+        synth.write_fcidump(path, args.phase_workload, seed=args.seed)
+        s = mc.CDFCI(mc.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
+                     z_threshold=args.z_threshold, threshold=0.0, groups=args.groups, device=local_rank)
+        s.reset()
+        s.run_iterations(args.warmup)
+        s.report()
+        s.leader_sections()
+        s.column_sections(enable=True)
+        n = args.steps
+        t = s.run_iterations_timed(n)
+        lead = s.leader_sections()
+        col = s.column_sections(enable=False)
+        rounds = max(col.pop("rounds"), 1)
+        ctas = max(col.pop("ctas"), 1)
+        merges = max(col.pop("merges"), 1)
+        per_cta = {"prelude": round(col.pop("prelude") / ctas), "post": round(col.pop("post") / ctas),
+                   "merge": round(col.pop("merge") / merges)}
+        scatter = []
+        if args.scatter_sweep:
+            for entries in (527072, 2108288, 8433152, 33732608):
+                for cps in (3, 8):
+                    for ilp in (1, 4):
+                        r = s.scatter_rate(entries, 10, ilp, cps)
+                        scatter.append({"slots": entries, "ctas_per_sm": cps, "ilp": ilp, "slots_per_s": r,
+                                        "us_per_launch": entries / r * 1e6})
+        rep = s.report()
+        groups = s.launch_info()["groups"]
+        s.close()
+    print(json.dumps({
+        "workload": args.phase_workload, "k": args.k, "m": args.m, "max_memory_gb": args.max_memory,
+        "warmup": args.warmup, "iterations": n, "groups": groups,
+        "leader_us_per_iteration": 1000.0 * t["leader_ms"] / n,
+        "column_us_per_iteration": 1000.0 * t["column_ms"] / n,
+        "leader_cycles_per_iteration": {k: round(v / n) for k, v in lead.items()},
+        "column_cycles_per_round": {k: round(v / rounds) for k, v in col.items()},
+        "column_cycles_per_cta": per_cta,
+        "column_rounds_per_cta": round(rounds / ctas, 2),
+        "energy": rep["energy"], "z_size": rep["z_size"],
+        "scatter_probe": scatter,
+    }, indent=1))
     return 0
 
 
@@ -517,6 +576,13 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.phases:
+        if world > 1 and rank != 0:
+            return 0
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        return phases_arm(args, local_rank)
     if args.workload == "curve":
         if world > 1 and rank != 0:
             return 0

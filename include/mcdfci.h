@@ -201,6 +201,13 @@ int mcd_batch_result(const mcd_batch* b, double* energies);
  * RHF FCIDUMPs only (MCD_ERR_UNSUPPORTED for UHF). */
 int mcd_rdm(mcd_solver* s, double* rdm1, double* rdm2);
 
+/* ||H c - E c|| / ||c|| of the current vector c = scale x, E = x'z / x'x,
+ * summed over the table's x and z (exact with z_threshold = 0, where z = H x
+ * on every connected determinant; with z_threshold > 0 the truncated z gives
+ * an estimate).  No counterpart in the reference, which reports only the
+ * residual of each subspace eigenproblem (src/solver.h:419-424). */
+int mcd_residual(mcd_solver* s, double* residual);
+
 /* ---- Checkpoint / restart -------------------------------------------------
  *
  * No counterpart in the reference.  mcd_checkpoint_save writes the
@@ -289,6 +296,11 @@ int mcd_debug_wavefunction(mcd_solver* s, uint64_t* alpha, uint64_t* beta, doubl
  * turns the timers on for later launches, 0 off (the default).  No
  * counterpart in the reference. */
 int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_t enable);
+/* Every occupied slot of the hash wavefunction (determinant, x, z), in slot
+ * order, after the end of the last iteration is applied; up to cap of them,
+ * *n_out receives the count.  No counterpart in the reference. */
+int mcd_debug_slots(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, double* z, int64_t cap,
+                    int64_t* n_out);
 /* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);
 

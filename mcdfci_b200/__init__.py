@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
-    "mcd_debug_column_sections",
+    "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots",
 )
 
 
@@ -159,6 +159,8 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
     L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
     L.mcd_debug_leader_sections.argtypes = [vp, _u64p, ctypes.c_int32]
+    L.mcd_residual.argtypes = [vp, _dp]
+    L.mcd_debug_slots.argtypes = [vp, _u64p, _u64p, _dp, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
 
@@ -461,6 +463,28 @@ class CDFCI:
                                         h.ctypes.data_as(_dp)))
         return h.reshape(k, k)
 
+    def residual(self) -> float:
+        """||H c - E c|| / ||c|| of the current vector (mcd_residual)."""
+        r = ctypes.c_double()
+        _check(library().mcd_residual(self._h, ctypes.byref(r)))
+        return r.value
+
+    def slots(self):
+        """(alpha, beta, x, z) of every occupied slot, in slot order."""
+        import numpy as np
+
+        cnt = ctypes.c_int64()
+        _check(library().mcd_debug_slots(self._h, None, None, None, None, 0, ctypes.byref(cnt)))
+        n = cnt.value
+        a = np.zeros(max(n, 1), dtype=np.uint64)
+        b = np.zeros(max(n, 1), dtype=np.uint64)
+        x = np.zeros(max(n, 1))
+        z = np.zeros(max(n, 1))
+        _check(library().mcd_debug_slots(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
+                                         x.ctypes.data_as(_dp), z.ctypes.data_as(_dp), n, ctypes.byref(cnt)))
+        k = min(cnt.value, n)
+        return a[:k], b[:k], x[:k], z[:k]
+
     def table_sums(self) -> dict:
         xx, xz = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
         occ = ctypes.c_uint64()
@@ -576,15 +600,28 @@ class CDFCIBatch:
         return r.as_dict()
 
 
+def _eig_inputs(hsub, x, z):
+    """hsub as a contiguous k x k array and x, z of length k; ValueError
+    otherwise (the C side copies k*k and k doubles from these buffers)."""
+    import numpy as np
+
+    hsub = np.ascontiguousarray(hsub, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    z = np.ascontiguousarray(z, dtype=np.float64).reshape(-1)
+    if hsub.ndim != 2 or hsub.shape[0] != hsub.shape[1]:
+        raise ValueError(f"hsub must be a square matrix, got shape {hsub.shape}")
+    k = hsub.shape[0]
+    if x.shape[0] != k or z.shape[0] != k:
+        raise ValueError(f"x and z must have k = {k} elements, got {x.shape[0]} and {z.shape[0]}")
+    return hsub, x, z, k
+
+
 def debug_eig(hsub, x, z, xx, xz):
     """CoordinateUpdateEig on one subproblem (src/solver.h:333-609), on the GPU.
     xx, xz are (hi, lo) pairs.  Returns (dx, new_xx, new_scale, branch)."""
     import numpy as np
 
-    hsub = np.ascontiguousarray(hsub, dtype=np.float64)
-    k = hsub.shape[0]
-    x = np.ascontiguousarray(x, dtype=np.float64)
-    z = np.ascontiguousarray(z, dtype=np.float64)
+    hsub, x, z, k = _eig_inputs(hsub, x, z)
     dx = np.zeros(k)
     nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
     br = ctypes.c_int32()
@@ -600,10 +637,7 @@ def eig_update_static(hsub, x, z, xx, xz, stream=None):
     buffers are a static array in the library, k <= 128.  Same returns."""
     import numpy as np
 
-    hsub = np.ascontiguousarray(hsub, dtype=np.float64)
-    k = hsub.shape[0]
-    x = np.ascontiguousarray(x, dtype=np.float64)
-    z = np.ascontiguousarray(z, dtype=np.float64)
+    hsub, x, z, k = _eig_inputs(hsub, x, z)
     dx = np.zeros(max(k, 1))
     nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
     br = ctypes.c_int32()

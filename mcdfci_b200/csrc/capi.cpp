@@ -598,6 +598,31 @@ int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* oc
   });
 }
 
+int mcd_residual(mcd_solver* s, double* residual) {
+  return guarded([&] {
+    if (!s || !residual) return fail(MCD_ERR_INVALID, "NULL argument.");
+    *residual = s->impl->residual();
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_slots(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, double* z, int64_t cap,
+                    int64_t* n_out) {
+  return guarded([&] {
+    if (!s || !n_out) return fail(MCD_ERR_INVALID, "NULL argument.");
+    std::vector<mcd::Slot> v;
+    s->impl->slots(v);
+    *n_out = static_cast<int64_t>(v.size());
+    for (int64_t i = 0; i < cap && i < static_cast<int64_t>(v.size()); ++i) {
+      if (alpha) alpha[i] = v[i].a;
+      if (beta) beta[i] = v[i].b;
+      if (x) x[i] = v[i].x;
+      if (z) z[i] = v[i].z;
+    }
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n) {
   return guarded([&] {
     if (!s || !cycles) return fail(MCD_ERR_INVALID, "NULL argument.");

@@ -731,8 +731,9 @@ int column_groups(int entries, int k, int resident) {
   }
   // ... and at most 96: the last CTA of a column merges all of its CTAs'
   // lists at the end of the launch, so long columns take longer CTAs (the
-  // 271,945-entry columns of 42 orbitals, 24 + 24 electrons: 1074 us per
-  // launch of 64 columns with 355 CTAs each, 932 us with 89).
+  // 271,945-entry columns of 42 orbitals, 24 + 24 electrons, one sweep of
+  // 64-column launches: 1074 us per launch with 355 CTAs each, 957 us with
+  // the cap's 96, 932 us with 89).
   g = std::min(g, 96);
   return g < 1 ? 1 : g;
 }

@@ -58,6 +58,40 @@ __global__ void table_sums_kernel(const Slot* slots, size_t n, dd* partial, unsi
   }
 }
 
+// Residual of the stored vector: partial[b] = sum over block b's slots of
+// (z - e x)^2 and x^2 in double-double.  With z = H x (z_threshold = 0 keeps
+// every connected determinant), sqrt(sum (z - e x)^2 / sum x^2) with e =
+// x'z / x'x is ||H c - E c|| / ||c|| for the coefficients c = scale x.
+__global__ void table_resid_kernel(const Slot* slots, size_t n, dd e, dd* partial) {
+  __shared__ dd srr[32], sxx[32];
+  dd arr{0, 0}, axx{0, 0};
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Slot s = slots[i];
+    if (slot_vacant(s.a, s.b)) continue;
+    const dd r = dd_add_d(dd_neg(dd_mul_d(e, s.x)), s.z);
+    arr = dd_add(arr, dd_mul(r, r));
+    axx = dd_add(axx, dd_two_prod(s.x, s.x));
+  }
+  arr = warp_sum_dd(arr);
+  axx = warp_sum_dd(axx);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    srr[warp] = arr;
+    sxx[warp] = axx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dd t1{0, 0}, t2{0, 0};
+    for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) {
+      t1 = dd_add(t1, srr[w]);
+      t2 = dd_add(t2, sxx[w]);
+    }
+    partial[2 * blockIdx.x] = t1;
+    partial[2 * blockIdx.x + 1] = t2;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Compaction: the slots that survive (x != 0, or |z| above a limit) are
 // copied in slot order into a buffer (per-block counts, then per-block
@@ -694,13 +728,37 @@ unsigned long long GpuSolver::compact(double z_threshold) {
 // the candidate lists by determinant; loading rebuilds the table by insertion.
 
 namespace {
-constexpr char kCkptMagic[8] = {'M', 'C', 'D', 'F', 'C', 'I', 'K', '1'};
+constexpr char kCkptMagic[8] = {'M', 'C', 'D', 'F', 'C', 'I', 'K', '2'};
 struct CkptHeader {
   char magic[8];
-  int32_t nso, nelec, k, m;
+  int32_t nso, na, nb, k, m, pad;
   double ecore;
+  uint64_t ham_hash;  // FNV-1a over the bytes of the Hamiltonian tables
   uint64_t state_bytes, nslots, ncand;
 };
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+  const unsigned char* c = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= c[i];
+    h *= 0x100000001b3ull;
+  }
+  return h;
+}
+
+// Identifies the integrals a checkpoint was made with: the same FCIDUMP and
+// hamiltonian threshold give the same tables, bit for bit.
+uint64_t ham_fingerprint(const HamHost& h) {
+  uint64_t f = 0xcbf29ce484222325ull;
+  f = fnv1a(f, h.hdiag.data(), h.hdiag.size() * sizeof(double));
+  f = fnv1a(f, h.d2.data(), h.d2.size() * sizeof(double));
+  f = fnv1a(f, h.sh.data(), h.sh.size() * sizeof(double));
+  f = fnv1a(f, h.st.data(), h.st.size() * sizeof(double));
+  f = fnv1a(f, h.spres.data(), h.spres.size() * sizeof(uint64_t));
+  f = fnv1a(f, h.vss.data(), h.vss.size() * sizeof(double));
+  f = fnv1a(f, h.wab.data(), h.wab.size() * sizeof(double));
+  return fnv1a(f, &h.ecore, sizeof(double));
+}
 }  // namespace
 
 void GpuSolver::gather_slots(double zlim, std::vector<Slot>& out) {
@@ -738,6 +796,11 @@ void GpuSolver::gather_slots(double zlim, std::vector<Slot>& out) {
   cudaFree(d_out);
 }
 
+void GpuSolver::slots(std::vector<Slot>& out) {
+  read_state();
+  gather_slots(-1.0, out);
+}
+
 void GpuSolver::checkpoint_save(const std::string& path) {
   read_state();
   std::vector<Slot> slots;
@@ -759,10 +822,12 @@ void GpuSolver::checkpoint_save(const std::string& path) {
   CkptHeader h{};
   std::memcpy(h.magic, kCkptMagic, 8);
   h.nso = ham_.nso;
-  h.nelec = na_ + nb_;
+  h.na = na_;
+  h.nb = nb_;
   h.k = opt_.k;
   h.m = m;
   h.ecore = ham_.ecore;
+  h.ham_hash = ham_fingerprint(ham_);
   h.state_bytes = sizeof(IterState);
   h.nslots = slots.size();
   h.ncand = cand.size();
@@ -783,7 +848,8 @@ void GpuSolver::checkpoint_load(const std::string& path) {
   std::vector<Slot> slots, cand;
   bool ok = std::fread(&h, sizeof(h), 1, f) == 1;
   if (ok && std::memcmp(h.magic, kCkptMagic, 8) != 0) ok = false;
-  if (ok && (h.nso != ham_.nso || h.nelec != na_ + nb_ || h.k != opt_.k || h.m != opt_.m || h.ecore != ham_.ecore ||
+  if (ok && (h.nso != ham_.nso || h.na != na_ || h.nb != nb_ || h.k != opt_.k || h.m != opt_.m ||
+             h.ecore != ham_.ecore || h.ham_hash != ham_fingerprint(ham_) ||
              h.state_bytes != sizeof(IterState) || h.ncand != static_cast<uint64_t>(kMaxK) * opt_.m)) {
     std::fclose(f);
     throw McdError(MCD_ERR_INVALID, "the checkpoint " + path + " belongs to another problem or other options");
@@ -1003,6 +1069,27 @@ void GpuSolver::table_sums(dd* xx, dd* xz, unsigned long long* occupied) {
   *xx = a;
   *xz = b;
   *occupied = c;
+}
+
+double GpuSolver::residual() {
+  read_state();
+  const int nb = 148 * 4;
+  dd* dp = device_alloc<dd>(2 * nb, "residual");
+  std::vector<dd> hp(2 * nb);
+  const dd e = dd_div(h_state_.xz, h_state_.xx);
+  table_resid_kernel<<<nb, 256, 0, stream_>>>(d_slots_, capacity_, e, dp);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(hp.data(), dp, hp.size() * sizeof(dd), cudaMemcpyDeviceToHost, stream_);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(stream_);
+  cudaFree(dp);
+  check(err, "residual");
+  dd rr{0, 0}, xx{0, 0};
+  for (int i = 0; i < nb; ++i) {
+    rr = dd_add(rr, hp[2 * i]);
+    xx = dd_add(xx, hp[2 * i + 1]);
+  }
+  return std::sqrt(dd_to_d(rr) / dd_to_d(xx));
 }
 
 std::vector<unsigned long long> GpuSolver::column_sections(bool enable) {

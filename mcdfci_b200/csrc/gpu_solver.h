@@ -70,6 +70,12 @@ class GpuSolver {
   std::vector<std::pair<Det, double>> column(Det d);
   std::vector<double> hsub(const std::vector<Det>& dets);
   void table_sums(dd* xx, dd* xz, unsigned long long* occupied);
+  // ||H c - E c|| / ||c|| of the current vector, from the table's x and z
+  // (exact when z_threshold = 0, so that z = H x on every connected determinant).
+  double residual();
+  // Every occupied slot (determinant, x, z) in slot order, after the pending
+  // end of the last iteration.
+  void slots(std::vector<Slot>& out);
   std::vector<std::pair<Det, double>> picked();
   // Spin-summed spatial 1- and 2-RDM of the current wavefunction, normalised
   // (rdm1[P*n+Q] = sum_s <a+_{Ps} a_{Qs}>, rdm2[((P*n+Q)*n+R)*n+S] =

@@ -8,7 +8,7 @@
 //                            accumulate xz), refetches the candidates, picks the
 //                            next k coordinates, builds H_sub, solves the
 //                            (k+1)x(k+1) eigenproblem and applies x += dx;
-//   column_kernel   (k clusters of C CTAs) generates the k Hamiltonian columns
+//   column_kernel   (k x G CTAs, G per column) generates the k Hamiltonian columns
 //                            and applies z += H_col * dx to the hash table,
 //                            keeping each column's top-m candidates.
 //

@@ -1,5 +1,5 @@
 // Leader kernel: the serial part of one mCDFCI iteration, run by one CTA of
-// 1024 threads between two column-kernel launches.
+// 512 threads between two column-kernel launches.
 //
 //   finish iteration t-1   z[D_c] = new_z_c for the picked D_c (the exact
 //                          recompute that overwrites the accumulated z,
@@ -932,15 +932,38 @@ size_t leader_smem_bytes(int k, int m) {
   return pick > eig ? pick : eig;
 }
 
+namespace {
+
+// The dynamic shared-memory limit of a kernel is a per-device attribute:
+// each device's largest configured size is kept, and the attribute is set
+// (outside stream capture: the first launch on a device precedes it) when a
+// launch on the current device needs more.
+constexpr int kMaxDevices = 64;
+struct SmemLimit {
+  std::mutex mu;
+  size_t bytes[kMaxDevices] = {};
+};
+
+cudaError_t ensure_smem(const void* func, size_t bytes, SmemLimit& lim) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(lim.mu);
+  if (bytes <= lim.bytes[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e == cudaSuccess) lim.bytes[dev] = bytes;
+  return e;
+}
+
+SmemLimit g_leader_smem, g_leader_batch_smem;
+
+}  // namespace
+
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s) {
   const size_t bytes = leader_smem_bytes(a.k_req, a.m);
-  static size_t configured = 0;
-  if (bytes > configured) {
-    cudaError_t e = cudaFuncSetAttribute(leader_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(bytes));
-    if (e != cudaSuccess) return e;
-    configured = bytes;
-  }
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(leader_kernel), bytes, g_leader_smem);
+  if (e != cudaSuccess) return e;
   leader_kernel<<<1, kLT, bytes, s>>>(a);
   return cudaGetLastError();
 }
@@ -948,13 +971,8 @@ cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s) {
 cudaError_t launch_leader_batch(const LeaderBatch& b, cudaStream_t s) {
   if (b.n < 1 || b.n > kMaxBatch) return cudaErrorInvalidValue;
   const size_t bytes = leader_smem_bytes(b.L[0].k_req, b.L[0].m);
-  static size_t configured = 0;
-  if (bytes > configured) {
-    cudaError_t e = cudaFuncSetAttribute(leader_kernel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(bytes));
-    if (e != cudaSuccess) return e;
-    configured = bytes;
-  }
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(leader_kernel_batch), bytes, g_leader_batch_smem);
+  if (e != cudaSuccess) return e;
   leader_kernel_batch<<<b.n, kLT, bytes, s>>>(b);
   return cudaGetLastError();
 }
@@ -1028,29 +1046,20 @@ __global__ void __launch_bounds__(kLT, 1) static_eig_kernel(int k, double* base,
   }
 }
 
-constexpr int kStaticEigMaxDevices = 64;
-std::mutex g_static_eig_mutex;
-double* g_static_eig_base[kStaticEigMaxDevices] = {};
-
-// Once per device, with that device current: the address of the array in
-// this device's copy of the module, and the shared-memory attribute of the
-// kernel for the largest k.
+// Set-up, with the device current: the address of the array in this
+// device's copy of the module, and the kernel's shared-memory attribute for
+// the largest k.  Both are looked up on every call (neither allocates, and
+// after the first call on a device the module is loaded, so they are cheap),
+// so that no address outlives the context it belongs to (a cudaDeviceReset
+// between two calls gives the second a fresh one).
 cudaError_t static_eig_setup(double** base) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_eig_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kStaticEigMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_static_eig_mutex);
-  if (!g_static_eig_base[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_static_eig_scratch);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(static_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(eig_work_doubles(kStaticEigMaxK) * sizeof(double)));
-    if (e != cudaSuccess) return e;
-    g_static_eig_base[dev] = static_cast<double*>(p);
-  }
-  *base = g_static_eig_base[dev];
+  e = cudaFuncSetAttribute(static_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(eig_work_doubles(kStaticEigMaxK) * sizeof(double)));
+  if (e != cudaSuccess) return e;
+  *base = static_cast<double*>(p);
   return cudaSuccess;
 }
 

@@ -151,3 +151,24 @@ class Oracle:
     def column_ab(self, a: int, b: int):
         words, vals = self.column(ab_to_interleaved(a, b, self.nw))
         return [interleaved_to_ab(w, self.nw) for w in words], vals
+
+    def column_ab_arrays(self, a: int, b: int):
+        """get_column of (a, b) as numpy arrays (alpha, beta, value), for at
+        most 64 spatial orbitals (two interleaved words)."""
+        words, vals = self.column(ab_to_interleaved(a, b, self.nw))
+        alpha = np.zeros(len(vals), dtype=np.uint64)
+        beta = np.zeros(len(vals), dtype=np.uint64)
+        for t in range(min(self.nw, 2)):
+            w = words[:, t]
+            alpha |= _compact_even(w) << np.uint64(32 * t)
+            beta |= _compact_even(w >> np.uint64(1)) << np.uint64(32 * t)
+        return alpha, beta, vals
+
+
+def _compact_even(w):
+    """Bits 0, 2, 4, ... of each uint64 packed into bits 0..31."""
+    x = w & np.uint64(0x5555555555555555)
+    for shift, mask in ((1, 0x3333333333333333), (2, 0x0F0F0F0F0F0F0F0F), (4, 0x00FF00FF00FF00FF),
+                        (8, 0x0000FFFF0000FFFF), (16, 0x00000000FFFFFFFF)):
+        x = (x | (x >> np.uint64(shift))) & np.uint64(mask)
+    return x

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference checkout (default /root/reference)
-after ``make -C oracle ref``:
+Run in a container that has the reference checkout, after
+``make -C oracle ref REF=<checkout>``:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <checkout>   (or MCDFCI_REFERENCE=<checkout>)
 
 It uses oracle/_ref/ref_dump (oracle/ref_dump.cpp compiled against the
 reference headers) and oracle/_ref/cdfci_omp (the reference solver compiled
@@ -110,11 +110,14 @@ def write_input(path, fcidump, **kw):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MCDFCI_REFERENCE"),
+                    help="the reference checkout (default: $MCDFCI_REFERENCE)")
     ap.add_argument("--only", choices=["all", "trajectories"], default="all")
     args = ap.parse_args()
     if args.only == "trajectories":
         return trajectories()
+    if not args.ref:
+        sys.exit("give the reference checkout: --ref <path> or MCDFCI_REFERENCE=<path>")
     for exe in (REF_DUMP, CDFCI):
         if not os.path.exists(exe):
             sys.exit(f"missing {exe}: run `make -C oracle ref` first")

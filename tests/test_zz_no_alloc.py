@@ -2,7 +2,8 @@
 a static device array of the library instead of per-call cudaMalloc.  It runs
 the same kernel as mcd_debug_eig, so each result is compared with
 mcd_debug_eig on the same inputs, on two calls in a row (the second call must
-not see anything left by the first).  Tolerance: dx, xx and scale within
+not see anything left by the first), and with the outputs the reference's
+CoordinateUpdateEig recorded on the same inputs.  Tolerance: dx, xx and scale within
 1e-12 relative (the kernels are the same; the tolerance only allows for a
 different reduction order should the two launch shapes ever differ).
 
@@ -57,6 +58,32 @@ def test_static_eig_matches_debug_eig_twice():
             assert _close(dx, ref[0]), (len(x), call)
             assert _close(nxx[0] + nxx[1], ref[1][0] + ref[1][1]), (len(x), call)
             assert _close(nsc[0] + nsc[1], ref[2][0] + ref[2][1]), (len(x), call)
+
+
+@pytest.mark.gpu
+def test_static_eig_matches_reference_records_twice():
+    """Against the reference itself: the outputs CoordinateUpdateEig produced
+    on subproblems recorded inside a reference solve (dx within 1e-9, xx and
+    |scale| within 1e-12 relative, the tolerances of the parity tests; the
+    first-iteration record's eigenvector sign is arbitrary in LAPACK)."""
+    for rec in load_golden("eig_h2o.json.gz")["calls"]:
+        k = rec["k"]
+        H = np.array(rec["hsub"]).reshape(k, k)
+        ref_dx = np.array(rec["dx"])
+        x = np.array(rec["x"])
+        for call in range(2):
+            dx, nxx, nsc, branch = m.eig_update_static(H, x, np.array(rec["z"]), tuple(rec["xx"]),
+                                                       tuple(rec["xz"]))
+            assert branch == (2 if rec["call"] == 0 else 1)
+            if branch == 2:
+                err = min(np.max(np.abs(dx - ref_dx)), np.max(np.abs(dx + ref_dx + 2 * x)))
+            else:
+                err = np.max(np.abs(dx - ref_dx) / (1.0 + np.abs(ref_dx)))
+            assert err < 1e-9, (rec["call"], call, err)
+            rxx = rec["new_xx"][0] + rec["new_xx"][1]
+            rsc = rec["new_scale"][0] + rec["new_scale"][1]
+            assert abs(nxx[0] + nxx[1] - rxx) <= 1e-12 * abs(rxx)
+            assert abs(abs(nsc[0] + nsc[1]) - abs(rsc)) <= 1e-12 * abs(rsc)
 
 
 @pytest.mark.gpu

@@ -243,6 +243,14 @@ int mcd_debug_hsub(mcd_solver* s, const uint64_t* alpha, const uint64_t* beta, i
  * and the branch (1: (k+1)x(k+1) problem, 2: k x k first-iteration problem). */
 int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                   const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch);
+/* mcd_debug_eig with the leader's first method: `drop` > 0 stands for the
+ * previous update's energy drop, so that shifted inverse iteration from a
+ * Cholesky factorisation of B - sigma I, sigma = xz/xx - max(16 drop, 1e-9
+ * (1 + |xz/xx|)), runs before the full reduction, as in a solve; *steps
+ * receives its steps, 0 when it fell back to the reduction.  Same outputs. */
+int mcd_debug_eig_shifted(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                          const double xz[2], double drop, double* dx, double new_xx[2], double new_scale[2],
+                          int32_t* branch, int32_t* steps);
 /* mcd_debug_eig without any allocation: no counterpart in the reference.
  * The same kernel and results, but its device buffers are a file-scope
  * static device array of 134 KB (k <= 128; a larger k returns
@@ -278,11 +286,12 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
  * No counterpart in the reference. */
 int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
                            double* slots_per_s);
-/* SM cycles spent in each phase of the leader kernel (16 phases: state load,
+/* SM cycles spent in each phase of the leader kernel (17 phases: state load,
  * finish, candidate gather, top-k, tie sort, picked, H_sub, update_x, publish,
  * eig setup, tridiagonalisation, multisection, inverse iteration,
- * back-transformation, Rayleigh quotient, eig finish), summed over launches
- * since the previous call, which resets them.  No counterpart in the reference. */
+ * back-transformation, Rayleigh quotient, eig finish, shifted inverse
+ * iteration), summed over launches since the previous call, which resets
+ * them.  No counterpart in the reference. */
 int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n);
 /* The determinants with nonzero x and their x (the coefficients are scale * x),
  * sorted by slot; up to cap of them, *n_out receives the count. */

@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
-    "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots",
+    "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
 )
 
 
@@ -137,6 +137,8 @@ def library() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_int32)]
     L.mcd_eig_update_static.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         ctypes.POINTER(ctypes.c_int32), vp]
+    L.mcd_debug_eig_shifted.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, ctypes.c_double, _dp, _dp, _dp,
+                                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
     L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
     L.mcd_debug_column_sections.argtypes = [vp, _u64p, ctypes.c_int32, ctypes.c_int32]
@@ -493,14 +495,14 @@ class CDFCI:
 
     LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
-                       "rayleigh", "eig_finish")
+                       "rayleigh", "eig_finish", "shifted")
 
     def leader_sections(self) -> dict:
         """SM cycles per leader-kernel phase since the previous call."""
         import numpy as np
 
-        v = np.zeros(16, dtype=np.uint64)
-        _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), 16))
+        v = np.zeros(len(self.LEADER_SECTIONS), dtype=np.uint64)
+        _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), len(v)))
         return {name: int(c) for name, c in zip(self.LEADER_SECTIONS, v)}
 
     def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1, ctas_per_sm: int = 0) -> float:
@@ -630,6 +632,24 @@ def debug_eig(hsub, x, z, xx, xz):
     _check(library().mcd_debug_eig(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
                                    xxa, xza, dx.ctypes.data_as(_dp), nxx, nsc, ctypes.byref(br)))
     return dx, tuple(nxx), tuple(nsc), br.value
+
+
+def debug_eig_shifted(hsub, x, z, xx, xz, drop):
+    """debug_eig with the shifted solver first, as the leader runs it when
+    the previous update's energy drop is known.  Returns (dx, new_xx,
+    new_scale, branch, steps); steps = 0 when the full reduction ran."""
+    import numpy as np
+
+    hsub, x, z, k = _eig_inputs(hsub, x, z)
+    dx = np.zeros(k)
+    nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+    br, st = ctypes.c_int32(), ctypes.c_int32()
+    xxa = (ctypes.c_double * 2)(*xx)
+    xza = (ctypes.c_double * 2)(*xz)
+    _check(library().mcd_debug_eig_shifted(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
+                                           z.ctypes.data_as(_dp), xxa, xza, float(drop), dx.ctypes.data_as(_dp),
+                                           nxx, nsc, ctypes.byref(br), ctypes.byref(st)))
+    return dx, tuple(nxx), tuple(nsc), br.value, st.value
 
 
 def eig_update_static(hsub, x, z, xx, xz, stream=None):

@@ -461,49 +461,83 @@ int mcd_debug_hsub(mcd_solver* s, const uint64_t* alpha, const uint64_t* beta, i
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// mcd_debug_eig / mcd_debug_eig_shifted: one eig update on the current device
+// from host buffers; the device buffers are released on every path.
+int debug_eig_host(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                   const double xz[2], double drop, double* dx, double new_xx[2], double new_scale[2],
+                   int32_t* branch, int32_t* steps) {
+  if (k < 1 || k > mcd::kMaxK) return fail(MCD_ERR_UNSUPPORTED, "k must be in 1..128.");
+  if (!hsub || !x || !z || !xx || !xz || !dx || !new_xx || !new_scale) return fail(MCD_ERR_INVALID, "NULL argument.");
+  struct Buffers {
+    double *h = nullptr, *x = nullptr, *z = nullptr, *dx = nullptr;
+    mcd::dd* out = nullptr;
+    int *br = nullptr, *steps = nullptr;
+    unsigned* err = nullptr;
+    ~Buffers() {
+      cudaFree(h);
+      cudaFree(x);
+      cudaFree(z);
+      cudaFree(dx);
+      cudaFree(out);
+      cudaFree(br);
+      cudaFree(steps);
+      cudaFree(err);
+    }
+  } b;
+  auto ck = [](cudaError_t e) {
+    if (e != cudaSuccess) throw mcd::McdError(MCD_ERR_CUDA, cudaGetErrorString(e));
+  };
+  ck(cudaMalloc(&b.h, sizeof(double) * k * k));
+  ck(cudaMalloc(&b.x, sizeof(double) * k));
+  ck(cudaMalloc(&b.z, sizeof(double) * k));
+  ck(cudaMalloc(&b.dx, sizeof(double) * k));
+  ck(cudaMalloc(&b.out, sizeof(mcd::dd) * 2));
+  ck(cudaMalloc(&b.br, sizeof(int)));
+  ck(cudaMalloc(&b.steps, sizeof(int)));
+  ck(cudaMalloc(&b.err, sizeof(unsigned)));
+  ck(cudaMemcpy(b.h, hsub, sizeof(double) * k * k, cudaMemcpyHostToDevice));
+  ck(cudaMemcpy(b.x, x, sizeof(double) * k, cudaMemcpyHostToDevice));
+  ck(cudaMemcpy(b.z, z, sizeof(double) * k, cudaMemcpyHostToDevice));
+  ck(cudaMemset(b.steps, 0, sizeof(int)));
+  ck(mcd::debug_eig(k, b.h, b.x, b.z, mcd::dd{xx[0], xx[1]}, mcd::dd{xz[0], xz[1]}, b.dx, b.out, b.br, b.err, 0,
+                    drop, b.steps));
+  mcd::dd out[2];
+  int br = 0, st = 0;
+  unsigned err = 0;
+  ck(cudaMemcpy(dx, b.dx, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  ck(cudaMemcpy(out, b.out, sizeof(out), cudaMemcpyDeviceToHost));
+  ck(cudaMemcpy(&br, b.br, sizeof(int), cudaMemcpyDeviceToHost));
+  ck(cudaMemcpy(&st, b.steps, sizeof(int), cudaMemcpyDeviceToHost));
+  ck(cudaMemcpy(&err, b.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  new_xx[0] = out[0].hi;
+  new_xx[1] = out[0].lo;
+  new_scale[0] = out[1].hi;
+  new_scale[1] = out[1].lo;
+  if (branch) *branch = br;
+  if (steps) *steps = st;
+  if (err) return fail(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
+  return MCD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                   const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch) {
+  return guarded([&] { return debug_eig_host(k, hsub, x, z, xx, xz, 0.0, dx, new_xx, new_scale, branch, nullptr); });
+}
+
+int mcd_debug_eig_shifted(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                          const double xz[2], double drop, double* dx, double new_xx[2], double new_scale[2],
+                          int32_t* branch, int32_t* steps) {
   return guarded([&] {
-    if (k < 1 || k > mcd::kMaxK) return fail(MCD_ERR_UNSUPPORTED, "k must be in 1..128.");
-    double *dh = nullptr, *dxv = nullptr, *dzv = nullptr, *ddx = nullptr;
-    mcd::dd* dout = nullptr;
-    int* dbr = nullptr;
-    unsigned* derr = nullptr;
-    auto ck = [](cudaError_t e) {
-      if (e != cudaSuccess) throw mcd::McdError(MCD_ERR_CUDA, cudaGetErrorString(e));
-    };
-    ck(cudaMalloc(&dh, sizeof(double) * k * k));
-    ck(cudaMalloc(&dxv, sizeof(double) * k));
-    ck(cudaMalloc(&dzv, sizeof(double) * k));
-    ck(cudaMalloc(&ddx, sizeof(double) * k));
-    ck(cudaMalloc(&dout, sizeof(mcd::dd) * 2));
-    ck(cudaMalloc(&dbr, sizeof(int)));
-    ck(cudaMalloc(&derr, sizeof(unsigned)));
-    ck(cudaMemcpy(dh, hsub, sizeof(double) * k * k, cudaMemcpyHostToDevice));
-    ck(cudaMemcpy(dxv, x, sizeof(double) * k, cudaMemcpyHostToDevice));
-    ck(cudaMemcpy(dzv, z, sizeof(double) * k, cudaMemcpyHostToDevice));
-    ck(mcd::debug_eig(k, dh, dxv, dzv, mcd::dd{xx[0], xx[1]}, mcd::dd{xz[0], xz[1]}, ddx, dout, dbr, derr, 0));
-    mcd::dd out[2];
-    int br = 0;
-    unsigned err = 0;
-    ck(cudaMemcpy(dx, ddx, sizeof(double) * k, cudaMemcpyDeviceToHost));
-    ck(cudaMemcpy(out, dout, sizeof(out), cudaMemcpyDeviceToHost));
-    ck(cudaMemcpy(&br, dbr, sizeof(int), cudaMemcpyDeviceToHost));
-    ck(cudaMemcpy(&err, derr, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    cudaFree(dh);
-    cudaFree(dxv);
-    cudaFree(dzv);
-    cudaFree(ddx);
-    cudaFree(dout);
-    cudaFree(dbr);
-    cudaFree(derr);
-    new_xx[0] = out[0].hi;
-    new_xx[1] = out[0].lo;
-    new_scale[0] = out[1].hi;
-    new_scale[1] = out[1].lo;
-    if (branch) *branch = br;
-    if (err) return fail(MCD_ERR_EIG, "The subspace eigenvalue problem failed.");
-    return MCD_OK;
+    if (!(drop > 0.0)) return fail(MCD_ERR_INVALID, "drop must be positive.");
+    return debug_eig_host(k, hsub, x, z, xx, xz, drop, dx, new_xx, new_scale, branch, steps);
   });
 }
 

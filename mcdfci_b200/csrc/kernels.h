@@ -62,6 +62,18 @@ struct IterState {
   int pending;                      // 1: the column kernel ran and its z reinsert / xz update is not applied yet
   unsigned long long emitted_total; // column entries over all iterations
   unsigned long long updates_total; // z updates over all iterations
+
+  // Subspace eigenproblem statistics (the [LOG] line).
+  double eig_drop;                  // last update's energy drop xz/xx - lambda (0: unknown)
+  double max_abs_evec;              // max |v_i|, i >= 1, of the last eigenvector
+  unsigned long long inv_updates;   // updates solved by shifted inverse iteration
+  unsigned long long inv_steps;     // their inverse-iteration steps, summed
+  unsigned long long eig_fallbacks; // shifted solves that fell back to the reduction
+  double inv_diff_sum;              // sum of the changes made by their last step
+  double inv_diff_max;
+  double inv_diff_curr;
+  int inv_steps_curr;               // steps of the last update (0: the reduction ran)
+  int pad2;
 };
 
 struct ColumnLaunch {
@@ -134,8 +146,9 @@ struct RdmLaunch {
 // 4 full sort when the k-th score is tied, 5 picked determinants, 6 H_sub,
 // 7 update_x, 8 publish, 9 eig setup, 10 tridiagonalisation, 11 multisection,
 // 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
-// 15 eig finish.
-constexpr int kLeaderSections = 16;
+// 15 eig finish,
+// 16 shifted inverse iteration (when it runs, in place of 10-13).
+constexpr int kLeaderSections = 17;
 
 // Phases of the column kernel timed into ColumnLaunch::sect (thread 0 of each
 // CTA, summed): 0 entry decode and integral value, 1 slot probe, 2 x load,
@@ -186,8 +199,12 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
 // One eig update on given inputs (device pointers); writes dx[k], xx_scale[0] =
 // new xx, xx_scale[1] = new scale, the branch taken and an error word.  The
 // lower triangle of hsub is overwritten with its upper triangle.
+// drop > 0: the last update's energy drop, which lets the shifted solver run
+// first (as the leader does); *steps (device int) receives its steps, 0 when
+// the reduction ran.
 cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
-                      dd* xx_scale, int* branch, unsigned* err, cudaStream_t s);
+                      dd* xx_scale, int* branch, unsigned* err, cudaStream_t s, double drop = 0.0,
+                      int* steps = nullptr);
 size_t leader_smem_bytes(int k, int m);
 
 // debug_eig on HOST buffers with its device buffers in a file-scope device

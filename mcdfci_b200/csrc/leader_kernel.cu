@@ -156,21 +156,39 @@ struct EigResult {
   int branch;
   bool ok;
   double resid;
+  double lambda;     // the eigenvalue (Rayleigh quotient of the vector)
+  double max_evec;   // max |v_i| over i >= 1 (branch 1) or i >= 0 (branch 2)
+  int shift_steps;   // steps of the shifted solver, 0 when the reduction ran
+  double shift_diff; // change made by its last refinement step
+  bool fallback;     // the shifted solver was tried and the reduction ran instead
 };
 
 constexpr int kEigVecs = 18;
 
+// Shared scratch of eig_update: B (lda), 18 vectors, and for k + 1 <=
+// kShiftMaxN the explicit inverse of the shifted solver's Cholesky factor.
 __host__ __device__ constexpr size_t eig_work_doubles(int k) {
-  return static_cast<size_t>(k + 1) * eig_lda(k + 1) + kEigVecs * static_cast<size_t>(k + 1) + 64;
+  return static_cast<size_t>(k + 1) * eig_lda(k + 1) + kEigVecs * static_cast<size_t>(k + 1) +
+         (k + 1 <= kShiftMaxN ? static_cast<size_t>(k + 1) * eig_lda(k + 1) : 0) + 64;
 }
 
+// drop: the last update's energy drop E - lambda (0 = unknown).  When it is
+// known and B has at most kShiftMaxN rows, the shifted solver runs first with
+// sigma = E - max(16 drop, 1e-9 (1 + |E|)) below the current energy E = xz/xx
+// (an upper bound of lambda_1: the current vector lies in the subspace, and
+// its Rayleigh quotient there is xz/xx) and the current vector as the start;
+// the reduction runs when that fails or its residual is not below 1e-11
+// (1 + |lambda|).
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
-                                double* dx, double* work, SectionClock& clk) {
+                                double* dx, double* work, SectionClock& clk, double drop) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1, s_res;
   __shared__ int s_branch;
   __shared__ dd s_rq;
   EigResult res;
+  res.shift_steps = 0;
+  res.shift_diff = 0.0;
+  res.fallback = false;
 
   // B = [[b00, b'], [b, H]] in A (leading dimension lda); H's block at (1, 1)
   // also serves the first-iteration k x k problem.
@@ -197,14 +215,18 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   double* vhi = vec + 15 * vs;   // normalised eigenvector, hi part
   double* vlo = vec + 16 * vs;   // lo part
 
-  for (int idx = tid; idx < k * k; idx += blockDim.x) {
-    const int i = idx / k, j = idx - i * k;
-    if (i <= j) {
-      const double v = H[idx];
-      A[(i + 1) * lda + (j + 1)] = v;
-      A[(j + 1) * lda + (i + 1)] = v;
+  double* Li = vec + kEigVecs * vs;  // [(k+1) x lda] when k + 1 <= kShiftMaxN
+  auto fill_h = [&]() {
+    for (int idx = tid; idx < k * k; idx += blockDim.x) {
+      const int i = idx / k, j = idx - i * k;
+      if (i <= j) {
+        const double v = H[idx];
+        A[(i + 1) * lda + (j + 1)] = v;
+        A[(j + 1) * lda + (i + 1)] = v;
+      }
     }
-  }
+  };
+  fill_h();
   __syncthreads();
   // H x in double (dsymv, src/solver.h:355); x'x, x'z, x'Hx in double-double,
   // rounded where the reference works in double.
@@ -255,9 +277,32 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   clk.mark(9);
 
   double* Ae = branch == 1 ? A : A + lda + 1;
-  eig_lowest(Ae, lda, n, V, clk);
+  const double e_cur = dd_to_d(dd_div(xz, xx));
+  bool shifted = false;
+  if (branch == 1 && n <= kShiftMaxN && drop > 0.0) {
+    const double delta = fmax(16.0 * drop, 1e-9 * (1.0 + fabs(e_cur)));
+    for (int i = tid; i < n; i += blockDim.x) V.y[i] = i == 0 ? y1 : x[i - 1];
+    __syncthreads();
+    int steps = 0;
+    double diff = 0.0;
+    shifted = eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff);
+    res.shift_steps = shifted ? steps : 0;
+    res.shift_diff = shifted ? diff : 0.0;
+    if (!shifted) {
+      res.fallback = true;
+      fill_h();
+      for (int i = tid; i <= k; i += blockDim.x) {
+        A[i] = bvec[i];
+        A[i * lda] = bvec[i];
+      }
+      __syncthreads();
+    }
+  }
+  clk.mark(16);
+  if (!shifted) eig_lowest(Ae, lda, n, V, clk);
   clk.mark(13);
 
+  for (int attempt = 0; attempt < 2; ++attempt) {
   // B v in double, one row per warp (H is symmetric, so its rows are read).
   const double* y = V.y;
   for (int r = warp; r < n; r += kLW) {
@@ -308,12 +353,34 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     }
   }
   __syncthreads();
+  // A shifted solve whose residual is not small runs the reduction instead.
+  if (!shifted || s_res <= 1e-11 * (1.0 + fabs(dd_to_d(s_rq)))) break;
+  shifted = false;
+  res.shift_steps = 0;
+  res.shift_diff = 0.0;
+  res.fallback = true;
+  fill_h();
+  for (int i = tid; i <= k; i += blockDim.x) {
+    A[i] = bvec[i];
+    A[i * lda] = bvec[i];
+  }
+  __syncthreads();
+  eig_lowest(Ae, lda, n, V, clk);
+  }
   clk.mark(14);
   const dd rq = s_rq;
   const double lam = dd_to_d(rq);
   res.resid = s_res;
   res.branch = branch;
   res.ok = true;
+  res.lambda = lam;
+  {
+    double mv = 0.0;
+    if (warp == 0)
+      for (int i = lane + (branch == 1 ? 1 : 0); i < n; i += 32) mv = fmax(mv, fabs(vhi[i]));
+    for (int o = 16; o > 0; o >>= 1) mv = fmax(mv, __shfl_xor_sync(~0u, mv, o));
+    res.max_evec = mv;  // warp 0's value; thread 0 publishes it
+  }
 
   if (branch == 1) {
     // lambda_q = -rq, gamma = v0 / y1, scale = gamma sqrt(lambda_q),
@@ -781,7 +848,7 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
     for (int t = tid; t < k * k; t += kLT) L.hsub_out[t] = Hs[t];
 
   // 6. Eig update.
-  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk);
+  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, sS.eig_drop);
   clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {
@@ -823,6 +890,20 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
     G->dx_max = mx;
     G->eig_residual_max = fmax(sS.eig_residual_max, er.resid);
     G->last_branch = er.branch;
+    // Energy drop of this update, for the next one's shift: the current
+    // energy xz/xx minus the eigenvalue (the energy after the update).
+    const double drop = dd_to_d(dd_div(sS.xz, sS.xx)) - er.lambda;
+    G->eig_drop = er.branch == 1 ? fmax(drop, 1e-300) : 0.0;
+    G->max_abs_evec = er.max_evec;
+    G->inv_steps_curr = er.shift_steps;
+    G->inv_diff_curr = er.shift_diff;
+    if (er.shift_steps > 0) {
+      G->inv_updates = sS.inv_updates + 1;
+      G->inv_steps = sS.inv_steps + er.shift_steps;
+      G->inv_diff_sum = sS.inv_diff_sum + er.shift_diff;
+      G->inv_diff_max = fmax(sS.inv_diff_max, er.shift_diff);
+    }
+    if (er.fallback) G->eig_fallbacks = sS.eig_fallbacks + 1;
     G->emitted = 0;
     G->updates = 0;
     G->iter = sS.iter + 1;
@@ -902,7 +983,7 @@ __device__ void symmetrise_from_upper(double* H, int k) {
 
 __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, const double* x, const double* z,
                                                            dd xx, dd xz, double* dx, dd* out, int* branch,
-                                                           unsigned* err) {
+                                                           unsigned* err, double drop, int* steps) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
   for (int i = threadIdx.x; i < k; i += blockDim.x) {
@@ -911,13 +992,14 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, con
   }
   symmetrise_from_upper(H, k);
   SectionClock clk{nullptr, 0};
-  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
+  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, drop);
   for (int i = threadIdx.x; i < k; i += blockDim.x) dx[i] = s_dx[i];
   if (threadIdx.x == 0) {
     out[0] = er.xx;
     out[1] = er.scale;
     *branch = er.branch;
     *err = er.ok ? 0u : kErrEig;
+    if (steps) *steps = er.shift_steps;
   }
 }
 
@@ -993,12 +1075,12 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
 }
 
 cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
-                      dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s) {
+                      dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s, double drop, int* steps) {
   const size_t bytes = eig_work_doubles(k) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(debug_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(bytes));
   if (e != cudaSuccess) return e;
-  debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err);
+  debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err, drop, steps);
   return cudaGetLastError();
 }
 
@@ -1034,7 +1116,8 @@ __global__ void __launch_bounds__(kLT, 1) static_eig_kernel(int k, double* base,
   }
   symmetrise_from_upper(base + kStaticEigH, k);
   SectionClock clk{nullptr, 0};
-  const EigResult er = eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk);
+  const EigResult er =
+      eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, 0.0);
   for (int i = threadIdx.x; i < k; i += blockDim.x) base[kStaticEigDx + i] = s_dx[i];
   if (threadIdx.x == 0) {
     dd* out = reinterpret_cast<dd*>(base + kStaticEigOut);

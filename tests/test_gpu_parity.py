@@ -132,6 +132,40 @@ def test_eig_update_vs_reference_fixture(fixture):
         assert abs(abs(_dd(nsc)) - abs(_dd(rec["new_scale"]))) <= 1e-12 * abs(_dd(rec["new_scale"]))
 
 
+@pytest.mark.parametrize("fixture", ["eig_h2o.json.gz", "eig_n7.json.gz"])
+def test_eig_update_shifted_vs_reference_fixture(fixture):
+    """The leader's first method on the recorded reference calls: shifted
+    inverse iteration from a Cholesky factorisation of B - sigma I, with the
+    drop a solve would pass (the energy drop of the update itself, read from
+    the record: xz/xx - lambda, lambda = -new_xx new_scale^2).  Same
+    tolerances as the full reduction; a drop far too small puts sigma above
+    lambda_1, the factorisation fails and the reduction gives the result."""
+    g = load_golden(fixture)
+    taken = 0
+    n = 0
+    for rec in g["calls"]:
+        if rec["call"] == 0:
+            continue
+        k = rec["k"]
+        H = np.array(rec["hsub"]).reshape(k, k)
+        lam = -_dd(rec["new_xx"]) * _dd(rec["new_scale"]) ** 2
+        drop = _dd(rec["xz"]) / _dd(rec["xx"]) - lam
+        for d, expect_shift in ((max(drop, 1e-12), True), (1e-300, False)):
+            dx, nxx, nsc, branch, steps = m.debug_eig_shifted(H, rec["x"], rec["z"], rec["xx"], rec["xz"], d)
+            assert branch == 1
+            if expect_shift:
+                n += 1
+                taken += steps > 0
+            ref_dx = np.array(rec["dx"])
+            err = np.max(np.abs(dx - ref_dx) / (1.0 + np.abs(ref_dx)))
+            assert err < 1e-9, (rec["call"], d, steps, err)
+            assert abs(_dd(nxx) - _dd(rec["new_xx"])) <= 1e-12 * abs(_dd(rec["new_xx"])), (rec["call"], steps)
+            assert abs(abs(_dd(nsc)) - abs(_dd(rec["new_scale"]))) <= 1e-12 * abs(_dd(rec["new_scale"]))
+    # the shifted solver, not its fallback, handles the recorded calls but
+    # the first few (an energy drop near the spectral gap)
+    assert taken >= n - 2, (taken, n)
+
+
 def _eig_reference_numpy(H, x, z, xx, xz):
     """The reference's eig update (src/solver.h:333-609) restated with numpy
     eigh in float64."""
@@ -170,6 +204,36 @@ def test_eig_update_random_vs_numpy(k):
     assert np.max(np.abs(dx - rdx) / (1 + np.abs(rdx))) < 1e-9
     assert abs(_dd(nxx) - rxx) < 1e-10 * abs(rxx)
     assert abs(_dd(nsc) - rsc) < 1e-10 * abs(rsc)
+
+
+@pytest.mark.parametrize("k", [1, 2, 8, 32, 33, 64])
+def test_eig_update_shifted_random_vs_numpy(k):
+    """Shifted solver on random subproblems near convergence: B is chosen
+    first, the current vector is its lowest eigenvector plus 1e-3 noise, and
+    (H, x, z, xx, xz) are derived so that the update rebuilds that B.  With
+    the exact energy drop and with 30 times it (a lower shift, more steps)."""
+    rng = np.random.default_rng(300 + k)
+    A = rng.normal(size=(k + 1, k + 1))
+    M = 0.05 * (A + A.T) / 2 - 30 * np.eye(k + 1) + np.diag(rng.uniform(0, 5, k + 1))
+    M[0, 0] = -33.0
+    w, U = np.linalg.eigh(M)
+    u = U[:, 0] * np.sign(U[0, 0])
+    y1 = 1.3 * u[0]
+    x = 1.3 * u[1:] + 1e-3 * rng.normal(size=k)
+    H = M[1:, 1:]
+    z = H @ x + y1 * M[0, 1:]
+    xx = float(y1 * y1 + x @ x)
+    xz = float(M[0, 0] * y1 * y1 + 2 * (x @ z) - x @ H @ x)
+    rdx, rxx, rsc = _eig_reference_numpy(H, x, z, xx, xz)
+    drop = xz / xx + rxx * rsc ** 2
+    assert drop > 0
+    for d in (drop, 30 * drop):
+        dx, nxx, nsc, branch, steps = m.debug_eig_shifted(H, x, z, (xx, 0.0), (xz, 0.0), d)
+        assert branch == 1
+        assert steps > 0
+        assert np.max(np.abs(dx - rdx) / (1 + np.abs(rdx))) < 1e-9
+        assert abs(_dd(nxx) - rxx) < 1e-10 * abs(rxx)
+        assert abs(abs(_dd(nsc)) - abs(rsc)) < 1e-10 * abs(rsc)
 
 
 @pytest.mark.parametrize("k", [1, 4, 16])

@@ -88,6 +88,14 @@ typedef struct mcd_options {
    * and the entries with x = 0 and |z scale| <= z_threshold are removed, until
    * it is below 40%, instead of failing with MCD_ERR_OVERFLOW.  0 by default. */
   int32_t compaction;
+  /* 1 (default): the hash table starts at the size two 64-iteration chunks
+   * of worst-case inserts need (k whole columns per iteration, kept below 3/4
+   * full) and doubles, rehashing into a new allocation between chunks, up to
+   * the table max_memory gives; occupancy limits and results are those of the
+   * full table.  0: the full table is allocated at creation, as the reference
+   * reserves its table.  A growth that finds the device memory taken by
+   * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
+  int32_t table_growth;
 } mcd_options;
 
 /* One line of the reference's report table (src/solver.h:761-798). */
@@ -274,6 +282,14 @@ int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied);
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
+/* The hash table: slots now, slots at full size (max_memory), growths so far. */
+int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_capacity, int32_t* growths);
+/* Host wall time of the solver's set-up stages in milliseconds, up to n of
+ * them: 0 Hamiltonian tables and reference determinant (host), 1 device
+ * allocations at creation, 2 table upload, 3 table fill of the last reset
+ * (synchronised), 4 CUDA graph builds, 5 table growths, 6 report read-backs,
+ * summed since creation.  No counterpart in the reference. */
+int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n);
 /* Launch shape of the column kernel: CTAs per column, length of the per-CTA
  * candidate lists, and entries per Hamiltonian column.  No counterpart in the
  * reference (it has no GPU launch). */

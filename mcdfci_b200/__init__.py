@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
+    "mcd_debug_table_info", "mcd_debug_setup_times",
 )
 
 
@@ -75,6 +76,7 @@ class mcd_options(ctypes.Structure):
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
+        ("table_growth", ctypes.c_int32),
     ]
 
 
@@ -162,6 +164,8 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
     L.mcd_debug_leader_sections.argtypes = [vp, _u64p, ctypes.c_int32]
     L.mcd_residual.argtypes = [vp, _dp]
+    L.mcd_debug_table_info.argtypes = [vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_debug_setup_times.argtypes = [vp, _dp, ctypes.c_int32]
     L.mcd_debug_slots.argtypes = [vp, _u64p, _u64p, _dp, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
@@ -281,7 +285,7 @@ def make_options(**kw) -> mcd_options:
     """mcd_options with the reference defaults, then keyword overrides
     (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
     z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
-    ("eig"|"ls"), groups, verbose, stream, device)."""
+    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth)."""
     o = mcd_options()
     library().mcd_options_default(ctypes.byref(o))
     occ = kw.pop("ref_det_occ", None)
@@ -293,8 +297,8 @@ def make_options(**kw) -> mcd_options:
             o.stream = ctypes.c_void_p(int(v) if v else 0)
         elif k == "z_threshold_search":
             o.z_threshold_search = int(bool(v))
-        elif k == "compaction":
-            o.compaction = int(bool(v))
+        elif k in ("compaction", "table_growth"):
+            setattr(o, k, int(bool(v)))
         else:
             setattr(o, k, v)
     if occ:
@@ -464,6 +468,19 @@ class CDFCI:
         _check(library().mcd_debug_hsub(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p), k,
                                         h.ctypes.data_as(_dp)))
         return h.reshape(k, k)
+
+    SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports")
+
+    def table_info(self) -> dict:
+        c, mc, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
+        _check(library().mcd_debug_table_info(self._h, ctypes.byref(c), ctypes.byref(mc), ctypes.byref(g)))
+        return {"capacity": c.value, "max_capacity": mc.value, "growths": g.value}
+
+    def setup_times(self) -> dict:
+        """Host wall time of the set-up stages (ms), summed since creation."""
+        v = (ctypes.c_double * len(self.SETUP_STAGES))()
+        _check(library().mcd_debug_setup_times(self._h, v, len(v)))
+        return {k: float(x) for k, x in zip(self.SETUP_STAGES, v)}
 
     def residual(self) -> float:
         """||H c - E c|| / ||c|| of the current vector (mcd_residual)."""

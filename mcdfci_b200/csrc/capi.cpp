@@ -71,6 +71,7 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.coordinate_update = o->coordinate_update;
   s.groups = o->groups;
   s.compaction = o->compaction != 0;
+  s.table_growth = o->table_growth != 0;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -154,6 +155,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   o->threshold = option.at("hamiltonian").at("threshold").as_number("hamiltonian:threshold");
   if (cd.has("groups")) o->groups = static_cast<int32_t>(cd.at("groups").as_number("groups"));
   if (cd.has("compaction")) o->compaction = cd.at("compaction").as_bool("compaction") ? 1 : 0;
+  if (cd.has("table_growth")) o->table_growth = cd.at("table_growth").as_bool("table_growth") ? 1 : 0;
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -189,6 +191,7 @@ void mcd_options_default(mcd_options* o) {
   o->coordinate_update = MCD_UPDATE_EIG;
   o->groups = 0;
   o->compaction = 0;
+  o->table_growth = 1;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;
@@ -680,6 +683,24 @@ int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t
   return guarded([&] {
     if (!s || !slots_per_s) return fail(MCD_ERR_INVALID, "NULL argument.");
     *slots_per_s = s->impl->scatter_rate(entries, reps, ilp, ctas_per_sm);
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_capacity, int32_t* growths) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    if (capacity) *capacity = static_cast<uint64_t>(s->impl->table_capacity());
+    if (max_capacity) *max_capacity = static_cast<uint64_t>(s->impl->table_max_capacity());
+    if (growths) *growths = s->impl->table_growths();
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n) {
+  return guarded([&] {
+    if (!s || !ms) return fail(MCD_ERR_INVALID, "NULL argument.");
+    for (int32_t i = 0; i < n && i < mcd::GpuSolver::kSetupStages; ++i) ms[i] = s->impl->setup_ms()[i];
     return MCD_OK;
   });
 }

@@ -55,6 +55,7 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       each.stream = G.stream;
       each.verbose = false;
       each.fill_gpu = false;  // the batch's columns fill the GPU together
+      each.table_growth = false;  // the batch launches its instances' kernels itself
       inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
       const int j = G.lb->n;
       G.lb->L[j] = inst_.back()->leader_launch();

@@ -162,6 +162,20 @@ __global__ void compact_reinsert_kernel(TableDev t, const Slot* src, size_t cnt)
   }
 }
 
+__global__ void rehash_kernel(const Slot* src, size_t n, TableDev t) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Slot s = src[i];
+    if (slot_vacant(s.a, s.b)) continue;
+    bool inserted;
+    const long long j = table_upsert(t, s.a, s.b, inserted);
+    if (j >= 0) {
+      t.slots[j].x = s.x;
+      t.slots[j].z = s.z;
+    }
+  }
+}
+
 // Candidate lists: (col < k_cur, i < cand_n[col]).  save: the slots'
 // contents; restore: find or insert each saved determinant, its new slot.
 __global__ void compact_cand_save_kernel(const Slot* slots, const IterState* st, const unsigned* cand_slot, int m,
@@ -189,6 +203,11 @@ __global__ void compact_cand_restore_kernel(TableDev t, const IterState* st, con
     }
     cand_slot[col * m + i] = static_cast<unsigned>(j);
   }
+}
+
+cudaError_t launch_rehash(const Slot* src, size_t n, const TableDev& t, cudaStream_t s) {
+  rehash_kernel<<<148 * 8, 256, 0, s>>>(src, n, t);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s) {
@@ -250,6 +269,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   uhf_ = fci.uhf;
   if (opt_.z_threshold_search && zt_ < 1e-10) zt_ = 1e-10;
 
+  using clock = std::chrono::steady_clock;
+  auto ms_since = [](clock::time_point t) { return std::chrono::duration<double, std::milli>(clock::now() - t).count(); };
+  auto t_host = clock::now();
   try {
     ham_ = build_hamiltonian(fci, opt_.threshold);
     std::string warning;
@@ -263,6 +285,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     throw McdError(MCD_ERR_INVALID, e.what());
   }
   ref_diag_ = diagonal_element(ham_, ref_);
+  setup_ms_[0] = ms_since(t_host);
   na_ = __builtin_popcountll(ref_.a);
   nb_ = __builtin_popcountll(ref_.b);
   if (na_ >= 64)  // its only determinant would carry the empty-slot key
@@ -278,9 +301,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   size_t pow2 = 8;
   while (static_cast<double>(pow2) * bytes_per_det < opt_.max_memory * 1073741824.0) pow2 *= 2;
   pow2 /= 2;
-  capacity_ = pow2;
+  max_capacity_ = pow2;
   max_size_ = static_cast<unsigned long long>(0.79 * static_cast<double>(pow2));
-  if (capacity_ > (1ull << 32))
+  if (max_capacity_ > (1ull << 32))
     throw McdError(MCD_ERR_UNSUPPORTED, "max_memory asks for more than 2^32 hash slots (128 GB).");
 
   // Device.
@@ -297,6 +320,25 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   groups_ = opt_.groups > 0 ? opt_.groups : column_groups(entries_, opt_.k, opt_.fill_gpu ? 3 * sms : 0);
   list_ = column_list_size(opt_.m);
 
+  // First table: large enough that two graphs' worth of iterations, each
+  // inserting at most k whole columns, keep it below 3/4 full, and at least
+  // 2^16 slots; the whole table when growth is off, or when the device could
+  // not hold this table and the full one at once (the last growth needs both).
+  {
+    size_t free_b = 0, total_b = 0;
+    check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t margin = static_cast<size_t>(1) << 30;
+    budget_slots_ = free_b > margin ? (free_b - margin) / sizeof(Slot) : 0;
+    const double per_chunk =
+        (2.0 * static_cast<double>(graph_iters_) * opt_.k + 1.0) * static_cast<double>(entries_);
+    size_t c = static_cast<size_t>(1) << 16;
+    while (c < max_capacity_ && 0.75 * static_cast<double>(c) < per_chunk) c <<= 1;
+    if (!opt_.table_growth || c >= max_capacity_ || c + max_capacity_ > budget_slots_) c = max_capacity_;
+    capacity_ = c;
+  }
+
+  auto t_alloc = clock::now();
+  double upload_ms = 0.0;
   try {
     // Hamiltonian tables in one allocation.
     const size_t n_hd = ham_.hdiag.size(), n_d2 = ham_.d2.size(), n_sh = ham_.sh.size(), n_st = ham_.st.size(),
@@ -356,6 +398,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     d_part_sum_ = device_alloc<double>(parts * kPartSum, "column partial sums");
     d_done_ = device_alloc<unsigned>(kMaxK, "column tickets");
     check(cudaMemsetAsync(d_done_, 0, kMaxK * sizeof(unsigned), stream_), "memset");
+    check(cudaMallocHost(&h_occ_, 2 * sizeof(unsigned long long)), "cudaMallocHost");
+    for (auto& e : ev_occ_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
   } catch (...) {
     release();
     throw;
@@ -391,7 +435,11 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.sect = d_sect_;
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
+  const auto t_up = clock::now();
   check(cudaStreamSynchronize(stream_), "table upload");
+  upload_ms = ms_since(t_up);
+  setup_ms_[1] = ms_since(t_alloc) - upload_ms;
+  setup_ms_[2] = upload_ms;
 }
 
 GpuSolver::~GpuSolver() { release(); }
@@ -426,15 +474,24 @@ void GpuSolver::release() {
   d_hsub_ = nullptr;
   d_err_ = nullptr;
   d_occ_ = nullptr;
+  if (h_occ_) cudaFreeHost(h_occ_);
+  h_occ_ = nullptr;
+  for (auto& e : ev_occ_) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   if (own_stream_ && stream_) cudaStreamDestroy(stream_);
   stream_ = nullptr;
   own_stream_ = false;
 }
 
 void GpuSolver::reset() {
+  const auto t0 = std::chrono::steady_clock::now();
   check(launch_table_fill(d_slots_, capacity_, stream_), "table fill");
   check(cudaMemsetAsync(d_err_, 0, sizeof(unsigned), stream_), "memset");
   check(cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_), "memset");
+  check(cudaStreamSynchronize(stream_), "table fill");
+  setup_ms_[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   std::memset(&h_state_, 0, sizeof(h_state_));
   h_state_.zt = zt_;
   h_state_.n_words = n_words_;
@@ -444,13 +501,17 @@ void GpuSolver::reset() {
   check(cudaMemcpyAsync(d_state_, &h_state_, sizeof(IterState), cudaMemcpyHostToDevice, stream_), "state upload");
   check(launch_init(ll_, ref_, ref_diag_, stream_), "init");
   check(launch_column(cl_, stream_), "column (init)");
+  // The initial column inserts at most one column's entries.
+  iters_enqueued_ = 0;
+  occ_iters_[0] = occ_iters_[1] = -1;
+  occ_exact_ = static_cast<unsigned long long>(entries_);
+  occ_exact_iters_ = 0;
 }
 
 void GpuSolver::build_graph() {
-  // Launch attributes are set on first use outside capture.
-  check(launch_leader(ll_, stream_), "leader");
-  check(launch_column(cl_, stream_), "column");
-  graph_iters_ = 64;
+  const auto t0 = std::chrono::steady_clock::now();
+  // Launch attributes are set outside the capture.
+  check(prepare_leader(ll_), "leader attributes");
   cudaGraph_t g = nullptr;
   check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
   for (long long i = 0; i < graph_iters_; ++i) {
@@ -460,47 +521,161 @@ void GpuSolver::build_graph() {
   check(cudaStreamEndCapture(stream_, &g), "end capture");
   check(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
   cudaGraphDestroy(g);
+  setup_ms_[4] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+size_t GpuSolver::next_capacity(size_t c) const {
+  size_t n = c * 2;
+  // The growth after this one would need this table and the full one at once.
+  if (n < max_capacity_ && n + max_capacity_ > budget_slots_) n = max_capacity_;
+  return std::min(n, max_capacity_);
+}
+
+void GpuSolver::record_occupancy(long long iters) {
+  iters_enqueued_ += iters;
+  if (capacity_ >= max_capacity_) return;
+  const int i = occ_next_;
+  check(cudaMemcpyAsync(h_occ_ + i, d_occ_, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+        "occupancy read");
+  check(cudaEventRecord(ev_occ_[i], stream_), "cudaEventRecord");
+  occ_iters_[i] = iters_enqueued_;
+  occ_next_ = 1 - i;
+}
+
+void GpuSolver::ensure_room(long long upcoming) {
+  if (capacity_ >= max_capacity_) return;
+  const double per_iter = static_cast<double>(opt_.k) * static_cast<double>(entries_);
+  // The newest occupancy known without waiting for the last chunk: the read
+  // after the chunk before it (usually done, since the last chunk is queued
+  // behind it), else the last synchronous read.
+  unsigned long long known = occ_exact_;
+  long long at = occ_exact_iters_;
+  const int older = occ_next_;  // a ring of two: the next slot to write holds the older read
+  if (occ_iters_[older] > at) {
+    check(cudaEventSynchronize(ev_occ_[older]), "occupancy wait");
+    known = h_occ_[older];
+    at = occ_iters_[older];
+  }
+  auto fits = [&](unsigned long long occ, long long iters, size_t cap) {
+    return static_cast<double>(occ) + static_cast<double>(iters) * per_iter <= 0.75 * static_cast<double>(cap);
+  };
+  if (fits(known, iters_enqueued_ - at + upcoming, capacity_)) return;
+  // Might not fit: wait for everything enqueued and grow until it does.
+  check(cudaStreamSynchronize(stream_), "synchronize");
+  unsigned long long occ = 0;
+  check(cudaMemcpy(&occ, d_occ_, sizeof(occ), cudaMemcpyDeviceToHost), "occupancy read");
+  occ_exact_ = occ;
+  occ_exact_iters_ = iters_enqueued_;
+  size_t cap = capacity_;
+  while (cap < max_capacity_ && !fits(occ, upcoming, cap)) cap = next_capacity(cap);
+  if (cap != capacity_) grow_to(cap);
+}
+
+void GpuSolver::grow_to(size_t new_capacity) {
+  const auto t0 = std::chrono::steady_clock::now();
+  read_state();  // applies the pending end of the iteration; nothing in flight
+  const int m = opt_.m;
+  Slot* fresh = nullptr;
+  Slot* saved = nullptr;
+  try {
+    fresh = device_alloc<Slot>(new_capacity, "hash wavefunction (growth)");
+    saved = device_alloc<Slot>(static_cast<size_t>(kMaxK) * m, "candidates");
+  } catch (const McdError& e) {
+    if (fresh) cudaFree(fresh);
+    throw McdError(MCD_ERR_CUDA, std::string("the hash table could not grow to ") + std::to_string(new_capacity) +
+                                     " slots (device memory taken since the solver was created?): " + e.what());
+  }
+  TableDev t = td_;
+  t.slots = fresh;
+  t.mask = new_capacity - 1;
+  t.max_probe = static_cast<int>(std::min<size_t>(new_capacity, 1u << 14));
+  cudaError_t e = launch_table_fill(fresh, new_capacity, stream_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_);
+  if (e == cudaSuccess) {
+    compact_cand_save_kernel<<<kMaxK, 128, 0, stream_>>>(d_slots_, d_state_, d_cand_slot_, m, saved);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = launch_rehash(d_slots_, capacity_, t, stream_);
+  if (e == cudaSuccess) {
+    compact_cand_restore_kernel<<<kMaxK, 128, 0, stream_>>>(t, d_state_, saved, d_cand_slot_, m);
+    e = cudaGetLastError();
+  }
+  unsigned long long occ = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&occ, d_occ_, sizeof(occ), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(saved);
+  if (e != cudaSuccess) {
+    cudaFree(fresh);
+    check(e, "table growth");
+  }
+  cudaFree(d_slots_);
+  d_slots_ = fresh;
+  capacity_ = new_capacity;
+  td_ = t;
+  cl_.tab = td_;
+  ll_.tab = td_;
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  ++growths_;
+  occ_exact_ = occ;
+  occ_exact_iters_ = iters_enqueued_;
+  occ_iters_[0] = occ_iters_[1] = -1;
+  setup_ms_[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  read_state();  // a probe-limit error during the rehash surfaces here
+}
+
+void GpuSolver::launch_chunk(long long n) {
+  if (n == graph_iters_) {
+    if (!graph_) build_graph();
+    check(cudaGraphLaunch(graph_, stream_), "graph launch");
+    return;
+  }
+  for (long long i = 0; i < n; ++i) {
+    check(launch_leader(ll_, stream_), "leader");
+    check(launch_column(cl_, stream_), "column");
+  }
 }
 
 void GpuSolver::run_iterations(long long n) {
-  if (n <= 0) return;
-  if (!graph_) {
-    build_graph();
-    --n;  // build_graph ran one iteration
-  }
-  while (n >= graph_iters_) {
-    check(cudaGraphLaunch(graph_, stream_), "graph launch");
-    n -= graph_iters_;
-  }
-  for (; n > 0; --n) {
-    check(launch_leader(ll_, stream_), "leader");
-    check(launch_column(cl_, stream_), "column");
+  while (n > 0) {
+    const long long c = std::min(n, graph_iters_);
+    ensure_room(c);
+    launch_chunk(c);
+    record_occupancy(c);
+    n -= c;
   }
 }
 
 void GpuSolver::run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms) {
   *leader_ms = *column_ms = *total_ms = 0.0;
   if (n <= 0) return;
-  std::vector<cudaEvent_t> ev(static_cast<size_t>(2 * n + 1));
+  // Per iteration: before the leader, between the kernels, after the column
+  // kernel; a table growth between two iterations counts in the total only.
+  std::vector<cudaEvent_t> ev(static_cast<size_t>(3 * n));
   for (auto& e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
   try {
-    check(cudaEventRecord(ev[0], stream_), "cudaEventRecord");
-    for (long long i = 0; i < n; ++i) {
-      check(launch_leader(ll_, stream_), "leader");
-      check(cudaEventRecord(ev[2 * i + 1], stream_), "cudaEventRecord");
-      check(launch_column(cl_, stream_), "column");
-      check(cudaEventRecord(ev[2 * i + 2], stream_), "cudaEventRecord");
+    for (long long i0 = 0; i0 < n; i0 += graph_iters_) {
+      const long long c = std::min(n - i0, graph_iters_);
+      ensure_room(c);
+      for (long long i = i0; i < i0 + c; ++i) {
+        check(cudaEventRecord(ev[3 * i], stream_), "cudaEventRecord");
+        check(launch_leader(ll_, stream_), "leader");
+        check(cudaEventRecord(ev[3 * i + 1], stream_), "cudaEventRecord");
+        check(launch_column(cl_, stream_), "column");
+        check(cudaEventRecord(ev[3 * i + 2], stream_), "cudaEventRecord");
+      }
+      record_occupancy(c);
     }
-    check(cudaEventSynchronize(ev[2 * n]), "cudaEventSynchronize");
+    check(cudaEventSynchronize(ev[3 * n - 1]), "cudaEventSynchronize");
     for (long long i = 0; i < n; ++i) {
       float a = 0.f, b = 0.f;
-      check(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]), "cudaEventElapsedTime");
-      check(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]), "cudaEventElapsedTime");
+      check(cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]), "cudaEventElapsedTime");
+      check(cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]), "cudaEventElapsedTime");
       *leader_ms += a;
       *column_ms += b;
     }
     float t = 0.f;
-    check(cudaEventElapsedTime(&t, ev[0], ev[2 * n]), "cudaEventElapsedTime");
+    check(cudaEventElapsedTime(&t, ev[0], ev[3 * n - 1]), "cudaEventElapsedTime");
     *total_ms = t;
   } catch (...) {
     for (auto& e : ev) cudaEventDestroy(e);
@@ -529,6 +704,7 @@ void GpuSolver::read_state() {
 }
 
 mcd_report GpuSolver::report() {
+  const auto t0 = std::chrono::steady_clock::now();
   read_state();
   mcd_report r{};
   r.iteration = h_state_.iter;
@@ -547,6 +723,9 @@ mcd_report GpuSolver::report() {
   r.occupied = 0;
   check(cudaMemcpy(&r.occupied, d_occ_, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "occupancy read");
   r.last_k = h_state_.k_cur;
+  occ_exact_ = r.occupied;
+  occ_exact_iters_ = iters_enqueued_;
+  setup_ms_[6] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return r;
 }
 
@@ -867,6 +1046,27 @@ void GpuSolver::checkpoint_load(const std::string& path) {
   if (slots.size() > limit)
     throw McdError(MCD_ERR_OVERFLOW, "The hash table is full. Please increase max_memory or z_threshold.");
   check(cudaStreamSynchronize(stream_), "synchronize");
+  // A table that grows on demand is enlarged first to hold the saved entries
+  // below 3/4 full (its contents are replaced anyway).
+  {
+    size_t cap = capacity_;
+    while (cap < max_capacity_ && static_cast<double>(slots.size()) > 0.75 * static_cast<double>(cap))
+      cap = next_capacity(cap);
+    if (cap != capacity_) {
+      Slot* fresh = device_alloc<Slot>(cap, "hash wavefunction (checkpoint)");
+      cudaFree(d_slots_);
+      d_slots_ = fresh;
+      capacity_ = cap;
+      td_.slots = fresh;
+      td_.mask = cap - 1;
+      td_.max_probe = static_cast<int>(std::min<size_t>(cap, 1u << 14));
+      cl_.tab = td_;
+      ll_.tab = td_;
+      if (graph_) cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+      ++growths_;
+    }
+  }
   Slot* d_in = device_alloc<Slot>(std::max<size_t>(slots.size(), 1), "checkpoint slots");
   Slot* d_saved = nullptr;
   try {
@@ -895,6 +1095,10 @@ void GpuSolver::checkpoint_load(const std::string& path) {
   cudaFree(d_in);
   cudaFree(d_saved);
   zt_ = st.zt;
+  iters_enqueued_ = 0;
+  occ_iters_[0] = occ_iters_[1] = -1;
+  occ_exact_ = slots.size();
+  occ_exact_iters_ = 0;
   read_state();
 }
 

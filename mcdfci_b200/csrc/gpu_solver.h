@@ -30,6 +30,10 @@ struct SolverOptions {
   int groups = 0;
   bool fill_gpu = true;  // with groups = 0: spread few columns over more CTAs (a batch fills the GPU itself)
   bool compaction = false;
+  // The hash table starts small and doubles (rehashing into a new
+  // allocation) as it fills, up to the size max_memory gives; false: the
+  // whole table is allocated at creation, as the reference reserves it.
+  bool table_growth = true;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -105,6 +109,15 @@ class GpuSolver {
   const HamHost& ham() const { return ham_; }
   Det reference_det() const { return ref_; }
   long long table_capacity() const { return static_cast<long long>(capacity_); }
+  long long table_max_capacity() const { return static_cast<long long>(max_capacity_); }
+  int table_growths() const { return growths_; }
+  // Host wall time of the set-up stages, in milliseconds (kSetupStages values):
+  // 0 Hamiltonian tables and reference determinant on the host, 1 device
+  // allocations of the constructor, 2 table upload, 3 table fill of the last
+  // reset (synchronised), 4 CUDA graph builds, 5 table growths, 6 report
+  // read-backs (finish, state copy, synchronisation), summed since creation.
+  static constexpr int kSetupStages = 7;
+  const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }
   // Launch descriptors and the column CTA count, for running this instance
@@ -123,6 +136,15 @@ class GpuSolver {
   void raise_device_error();
   void build_graph();
   void gather_slots(double zlim, std::vector<Slot>& out);  // occupied slots kept by zlim, in slot order
+  // Table growth: before `upcoming` iterations are enqueued, make sure that
+  // the table keeps its load below 3/4 even if every one of them inserts a
+  // whole column per coordinate, from the occupancy read (lagged by one
+  // chunk) after earlier chunks; grows, synchronously, when it might not.
+  void ensure_room(long long upcoming);
+  void grow_to(size_t new_capacity);        // rehash into a table of new_capacity slots
+  size_t next_capacity(size_t c) const;     // the capacity after c
+  void record_occupancy(long long iters);   // async occupancy read after a chunk of iters
+  void launch_chunk(long long n);           // n <= graph_iters_ iterations, graph or direct
 
   SolverOptions opt_;
   HamHost ham_;
@@ -130,7 +152,20 @@ class GpuSolver {
   double ref_diag_ = 0.0;
   int na_ = 0, nb_ = 0, entries_ = 0, groups_ = 1, list_ = 32, n_words_ = 1;
   bool uhf_ = false;
-  size_t capacity_ = 0;             // hash slots (power of two)
+  size_t capacity_ = 0;             // hash slots now (power of two)
+  size_t max_capacity_ = 0;         // hash slots max_memory gives (the reference's table)
+  size_t budget_slots_ = 0;         // device memory for two tables at once, in slots
+  int growths_ = 0;
+  double setup_ms_[kSetupStages] = {};
+  // Occupancy reads after the last two chunks: pinned host words, events, and
+  // the iterations enqueued since the reset when each was recorded.
+  unsigned long long* h_occ_ = nullptr;
+  cudaEvent_t ev_occ_[2] = {nullptr, nullptr};
+  long long occ_iters_[2] = {-1, -1};
+  int occ_next_ = 0;
+  long long iters_enqueued_ = 0;      // since the last reset
+  unsigned long long occ_exact_ = 0;  // occupancy read synchronously ...
+  long long occ_exact_iters_ = 0;     // ... after this many enqueued iterations
   unsigned long long max_size_ = 0; // reference max_wavefunction_size
   double zt_ = 0.0;
   double result_energy_ = 0.0;
@@ -158,7 +193,7 @@ class GpuSolver {
   IterState h_state_{};
 
   cudaGraphExec_t graph_ = nullptr;
-  long long graph_iters_ = 0;
+  static constexpr long long graph_iters_ = 64;
 };
 
 }  // namespace mcd

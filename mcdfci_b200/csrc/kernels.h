@@ -168,6 +168,9 @@ int column_list_size(int m);
 int column_groups(int entries, int k, int resident);
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
+// Sets, on the current device, the launch attribute launch_leader needs for
+// a (its dynamic shared-memory limit); for use before a stream capture.
+cudaError_t prepare_leader(const LeaderLaunch& a);
 cudaError_t launch_leader_batch(const LeaderBatch& b, cudaStream_t s);
 cudaError_t launch_column_batch(const ColumnBatch& b, cudaStream_t s);
 cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStream_t s);
@@ -175,6 +178,8 @@ cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStrea
 // determinants, xz += dot), so that reported energies and table contents are
 // those after a complete iteration.  Idempotent.
 cudaError_t launch_finish(const LeaderLaunch& a, cudaStream_t s);
+// Every occupied slot of `src` (n slots) inserted into table t with its x and z.
+cudaError_t launch_rehash(const Slot* src, size_t n, const TableDev& t, cudaStream_t s);
 // Table initialisation (all slots empty) and whole-table sums.
 cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s);
 cudaError_t launch_table_sums(const Slot* slots, size_t n, dd* partial, unsigned long long* count, int nblocks,

@@ -1042,6 +1042,10 @@ SmemLimit g_leader_smem, g_leader_batch_smem;
 
 }  // namespace
 
+cudaError_t prepare_leader(const LeaderLaunch& a) {
+  return ensure_smem(reinterpret_cast<const void*>(leader_kernel), leader_smem_bytes(a.k_req, a.m), g_leader_smem);
+}
+
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s) {
   const size_t bytes = leader_smem_bytes(a.k_req, a.m);
   cudaError_t e = ensure_smem(reinterpret_cast<const void*>(leader_kernel), bytes, g_leader_smem);

@@ -21,6 +21,10 @@ eigenproblem, apply x += dx and z += H_col * dx in the hash wavefunction.
                its average device time, against the measured HBM copy peak
   cpu_baseline the reference cdfci_omp, compiled from its sources, on a
                bounded sample of the same workload on this host's cores
+  aged         value's timing repeated after --aged-iterations iterations in
+               all, on the grown table (load factor stated)
+  e2e_detail   the end-to-end run's stages: host tables, device allocation,
+               upload, table fill, graph builds, growths, report read-backs
 
   batched      the 32-point dissociation curve (synthetic n16_5a5b points,
                k = m = 16, 1 GB table each): coordinate updates/s of all 32
@@ -81,6 +85,9 @@ def parse_args():
     ap.add_argument("--curve-iterations", type=int, default=20000)
     ap.add_argument("--curve-report", type=int, default=1000)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-curve throughput object")
+    ap.add_argument("--aged-iterations", type=int, default=2000,
+                    help="iterations in all before the aged-table timing (0: skip it)")
+    ap.add_argument("--aged-steps", type=int, default=256)
     ap.add_argument("--phases", action="store_true",
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
@@ -98,7 +105,8 @@ def config(args):
         "max_memory_gb": args.max_memory,
         "z_threshold": args.z_threshold,
         "step": "one mCDFCI iteration",
-        "l2": "inputs larger than L2: the hash wavefunction is 68.7 GB (2^31 slots x 32 B) vs 126 MB L2",
+        "l2": "inputs larger than L2: the hash wavefunction (at least 2^27 slots x 32 B = 4.3 GB, growing "
+              "as it fills up to 2^31 slots = 68.7 GB for 64 GB) vs 126 MB L2",
         "parallelism": "replicas",
     }
 
@@ -480,6 +488,31 @@ def b200_arm(args, rank, world, local_rank):
         # its slot (key, x, atomic z add of zero), 1 or 4 in flight per thread.
         per_launch = max(1, int(entries / args.steps))
         scatter = max(solver.scatter_rate(per_launch, 20, 1), solver.scatter_rate(per_launch, 20, 4))
+        table_main = solver.table_info()
+        # The same timing on an aged table: iterate on to --aged-iterations
+        # iterations in all (the table grows as it fills), then time the
+        # product path again.
+        aged = None
+        if args.aged_iterations > 0:
+            done = r1["iteration"]
+            if args.aged_iterations > done:
+                solver.run_iterations(args.aged_iterations - done)
+            ra0 = solver.report()
+            n_aged = args.aged_steps
+            ev0.record(ext)
+            solver.run_iterations(n_aged)
+            ev1.record(ext)
+            ev1.synchronize()
+            ra1 = solver.report()
+            ta = ev0.elapsed_time(ev1) / 1000.0
+            ti = solver.table_info()
+            aged = {"iterations_before": ra0["iteration"], "steps": n_aged, "ms_per_step": 1000.0 * ta / n_aged,
+                    "updates_per_s": args.k * n_aged / ta, "z_size": ra1["z_size"], "occupied": ra1["occupied"],
+                    "table_slots": ti["capacity"], "load_factor": ra1["occupied"] / ti["capacity"],
+                    "table_growths": ti["growths"], "energy": ra1["energy"],
+                    "entries_per_step": (ra1["emitted_total"] - ra0["emitted_total"]) / n_aged,
+                    "timing": "CUDA events on the solver's stream around the product path (graphs of 64 "
+                              "iterations), table growths inside the timed steps included"}
         solver.close()
 
         peak, peak_kind = hbm_peak()
@@ -490,6 +523,7 @@ def b200_arm(args, rank, world, local_rank):
                     "kernel": "column_kernel", "entries_per_launch": entries / args.steps,
                     "algorithmic_bytes_per_entry": BYTES_PER_ENTRY, "avg_launch_ms": col_ms_avg,
                     "leader_ms_per_step": t["leader_ms"] / args.steps,
+                    "table_slots": table_main["capacity"],
                     "scatter_ceiling": {"slots_per_s": scatter,
                                         "column_entries_per_s": (entries / args.steps) / (col_ms_avg / 1000.0),
                                         "frac": (entries / args.steps) / (col_ms_avg / 1000.0) / scatter,
@@ -535,6 +569,7 @@ def b200_arm(args, rank, world, local_rank):
                 "clocks": clocks,
                 "energy": r1["energy"],
                 "z_size": r1["z_size"],
+                "aged": aged,
                 "e2e_detail": e2e,
             }
             print(json.dumps(out))
@@ -553,10 +588,27 @@ def e2e_run(mc, fc, args, local_rank):
     s = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                  z_threshold=args.z_threshold, threshold=0.0, device=local_rank, num_iterations=iters,
                  report_interval=interval, groups=args.groups)
+    t_created = time.perf_counter()
     s.solve()
     energy = s.result_energy
     dt = time.perf_counter() - t0  # the result is in hand; releasing the solver is not part of it
+    stages = s.setup_times()
+    table = s.table_info()
     s.close()
+    create_ms = 1000.0 * (t_created - t0)
+    breakdown = {
+        "create_ms": create_ms,
+        "create_host_tables_ms": stages["host_tables"],
+        "create_device_alloc_ms": stages["device_alloc"],
+        "create_upload_ms": stages["upload"],
+        "solve_ms": 1000.0 * dt - create_ms,
+        "solve_table_fill_ms": stages["table_fill"],
+        "solve_graph_build_ms": stages["graph_build"],
+        "solve_table_growth_ms": stages["growth"],
+        "solve_report_readback_ms": stages["reports"],
+        "table_slots": table["capacity"], "table_slots_max": table["max_capacity"],
+        "table_growths": table["growths"],
+    }
     n = fc.norb
     nsp = n // 2
     table_bytes = 8 * (n + n * n + 2 * nsp * nsp + 2 * nsp * nsp * n + 2 * nsp + 2 * (nsp * (nsp - 1) // 2) ** 2 + nsp ** 4)
@@ -565,8 +617,10 @@ def e2e_run(mc, fc, args, local_rank):
     d2h = (iters // interval) * (state_bytes + 8)
     return {"value": args.k * iters / dt, "unit": UNIT, "h2d_bytes_per_step": h2d / iters,
             "d2h_bytes_per_step": d2h / iters, "seconds": dt, "iterations": iters, "energy": energy,
-            "what": "mcd_create_from_fcidump (Hamiltonian tables host->device, 64 GB table init) + mcd_solve "
-                    f"({iters} iterations, a report read back every {interval}) + mcd_result; mcd_destroy after the clock"}
+            "stages": breakdown,
+            "what": "mcd_create_from_fcidump (Hamiltonian tables host->device, hash table allocation) + mcd_solve "
+                    f"(table fill, {iters} iterations, a report read back every {interval}) + mcd_result; "
+                    "mcd_destroy after the clock"}
 
 
 def main():

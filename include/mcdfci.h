@@ -121,7 +121,10 @@ typedef struct mcd_report {
 typedef int (*mcd_report_cb)(const mcd_report* report, void* user);
 
 /* Called for each instance of a batch after every report_interval
- * iterations; return nonzero to stop the batch. */
+ * iterations; return MCD_CB_RETIRE to stop advancing that instance (it keeps
+ * its state, and the batch's later launches leave it out, so the others run
+ * on a smaller grid), any other nonzero value to stop the batch. */
+#define MCD_CB_RETIRE 2
 typedef int (*mcd_batch_report_cb)(int32_t instance, const mcd_report* report, void* user);
 
 /* ---- Input ------------------------------------------------------------- */
@@ -186,7 +189,8 @@ int mcd_batch_create(const mcd_fcidump* const* fcidumps, int32_t n, const mcd_op
 void mcd_batch_destroy(mcd_batch* b);
 int mcd_batch_size(const mcd_batch* b, int32_t* n);
 /* Initial state of every instance, then num_iterations iterations with a
- * report of each instance every report_interval (callback may be NULL). */
+ * report of each active instance every report_interval (callback may be
+ * NULL), until every instance is retired or num_iterations is reached. */
 int mcd_batch_solve(mcd_batch* b, mcd_batch_report_cb cb, void* user);
 int mcd_batch_reset(mcd_batch* b);
 int mcd_batch_run_iterations(mcd_batch* b, int64_t n);

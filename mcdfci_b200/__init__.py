@@ -29,6 +29,7 @@ MCD_ERR_CUDA = 4
 MCD_ERR_UNSUPPORTED = 5
 MCD_ERR_NO_CANDIDATES = 6
 MCD_STOPPED = 7
+MCD_CB_RETIRE = 2  # batch report callback: stop advancing this instance only
 MCD_PICK_GCD_GRAD = 0
 MCD_UPDATE_EIG = 1
 MCD_UPDATE_LS = 2
@@ -587,7 +588,12 @@ class CDFCIBatch:
         def cb(i, rep, _user):
             d = rep.contents.as_dict()
             self.reports[i].append(d)
-            return 1 if (callback is not None and callback(i, d)) else 0
+            if callback is None:
+                return 0
+            v = callback(i, d)
+            if v == "retire" or (not isinstance(v, bool) and v == MCD_CB_RETIRE):
+                return MCD_CB_RETIRE
+            return 1 if v else 0
 
         c = BATCH_REPORT_CB(cb)
         rc = library().mcd_batch_solve(self._h, c, None)

@@ -57,13 +57,10 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       each.fill_gpu = false;  // the batch's columns fill the GPU together
       each.table_growth = false;  // the batch launches its instances' kernels itself
       inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
-      const int j = G.lb->n;
-      G.lb->L[j] = inst_.back()->leader_launch();
-      G.cb->L[j] = inst_.back()->column_launch();
-      G.cb->cta_begin[j + 1] = G.cb->cta_begin[j] + inst_.back()->column_ctas();
-      G.lb->n = G.cb->n = j + 1;
     }
     energies_.assign(fcis.size(), 0.0);
+    active_.assign(fcis.size(), 1);
+    set_groups();
   } catch (...) {
     inst_.clear();
     for (size_t g = 0; g < groups_.size(); ++g)
@@ -96,12 +93,42 @@ void GpuBatch::join_streams() {
       if (g != h) check(cudaStreamWaitEvent(groups_[g].stream, join_[h], 0), "cudaStreamWaitEvent");
 }
 
+void GpuBatch::set_groups() {
+  const size_t ng = groups_.size();
+  for (Group& G : groups_) {
+    if (G.graph) cudaGraphExecDestroy(G.graph);
+    G.graph = nullptr;
+    G.lb->n = G.cb->n = 0;
+    G.cb->cta_begin[0] = 0;
+  }
+  for (size_t i = 0; i < inst_.size(); ++i) {
+    if (!active_[i]) continue;
+    Group& G = groups_[i % ng];
+    const int j = G.lb->n;
+    G.lb->L[j] = inst_[i]->leader_launch();
+    G.cb->L[j] = inst_[i]->column_launch();
+    G.cb->cta_begin[j + 1] = G.cb->cta_begin[j] + inst_[i]->column_ctas();
+    G.lb->n = G.cb->n = j + 1;
+  }
+}
+
+int GpuBatch::active() const {
+  int n = 0;
+  for (char a : active_) n += a ? 1 : 0;
+  return n;
+}
+
 void GpuBatch::reset() {
   for (auto& s : inst_) s->reset();
+  if (active() != size()) {
+    active_.assign(inst_.size(), 1);
+    set_groups();
+  }
   join_streams();
 }
 
 void GpuBatch::launch_iteration(Group& g) {
+  if (g.lb->n == 0) return;
   check(launch_leader_batch(*g.lb, g.stream), "batched leader");
   check(launch_column_batch(*g.cb, g.stream), "batched column");
 }
@@ -109,6 +136,7 @@ void GpuBatch::launch_iteration(Group& g) {
 void GpuBatch::build_graphs() {
   graph_iters_ = 64;
   for (Group& G : groups_) {
+    if (G.lb->n == 0) continue;
     launch_iteration(G);  // sets launch attributes outside capture
     cudaGraph_t g = nullptr;
     check(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -123,13 +151,16 @@ void GpuBatch::build_graphs() {
 }
 
 void GpuBatch::run_iterations(long long n) {
-  if (n <= 0) return;
-  if (!groups_[0].graph) {
+  if (n <= 0 || active() == 0) return;
+  bool built = false;
+  for (const Group& G : groups_) built = built || G.graph != nullptr;
+  if (!built) {
     build_graphs();
     --n;
   }
   while (n >= graph_iters_) {
-    for (Group& G : groups_) check(cudaGraphLaunch(G.graph, G.stream), "graph launch");
+    for (Group& G : groups_)
+      if (G.graph) check(cudaGraphLaunch(G.graph, G.stream), "graph launch");
     n -= graph_iters_;
   }
   for (; n > 0; --n)
@@ -142,8 +173,7 @@ void GpuBatch::run_iterations(long long n) {
 // the time is not split by kernel: leader_ms and column_ms stay 0.
 void GpuBatch::run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms) {
   *leader_ms = *column_ms = *total_ms = 0.0;
-  if (n <= 0) return;
-  if (!groups_[0].graph) build_graphs();
+  if (n <= 0 || active() == 0) return;
   cudaEvent_t a = nullptr, b = nullptr;
   check(cudaEventCreate(&a), "cudaEventCreate");
   check(cudaEventCreate(&b), "cudaEventCreate");
@@ -174,10 +204,11 @@ int GpuBatch::solve(int (*cb)(int, const mcd_report*, void*), void* user) {
   reset();
   const auto t0 = std::chrono::steady_clock::now();
   const long long chunks = opt_.num_iterations / opt_.report_interval;
-  for (long long c = 0; c < chunks; ++c) {
+  for (long long c = 0; c < chunks && active() > 0; ++c) {
     run_iterations(opt_.report_interval);
-    bool stop = false;
+    bool stop = false, retired = false;
     for (int i = 0; i < size(); ++i) {
+      if (!active_[static_cast<size_t>(i)]) continue;
       mcd_report r = report(i);
       r.time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       energies_[static_cast<size_t>(i)] = r.energy;
@@ -186,11 +217,19 @@ int GpuBatch::solve(int (*cb)(int, const mcd_report*, void*), void* user) {
                   << "  energy " << std::fixed << std::setprecision(10) << r.energy << "  |x|_0 " << r.x_size
                   << "  |z|_0 " << r.z_size << "  time " << std::setprecision(2) << r.time_s << std::endl;
       }
-      if (cb && cb(i, &r, user) != 0) stop = true;
+      const int rc = cb ? cb(i, &r, user) : 0;
+      if (rc == MCD_CB_RETIRE) {
+        active_[static_cast<size_t>(i)] = 0;
+        retired = true;
+      } else if (rc != 0) {
+        stop = true;
+      }
     }
     if (stop) return MCD_STOPPED;
+    if (retired) set_groups();
   }
-  for (int i = 0; i < size(); ++i) energies_[static_cast<size_t>(i)] = report(i).energy;
+  for (int i = 0; i < size(); ++i)
+    if (active_[static_cast<size_t>(i)]) energies_[static_cast<size_t>(i)] = report(i).energy;
   return MCD_OK;
 }
 

@@ -34,8 +34,13 @@ class GpuBatch {
   void run_iterations_timed(long long n, double* leader_ms, double* column_ms, double* total_ms);
   mcd_report report(int i);
   // num_iterations iterations of every instance, a report of each every
-  // report_interval; cb(instance, report) returning nonzero stops the batch.
+  // report_interval; cb(instance, report) returning MCD_CB_RETIRE stops that
+  // instance (it keeps its state and energy, and later launches leave it
+  // out), any other nonzero value stops the batch.  Ends when every
+  // instance is retired or num_iterations is reached.
   int solve(int (*cb)(int, const mcd_report*, void*), void* user);
+  // Instances still advanced by run_iterations (all of them after a reset).
+  int active() const;
   double result_energy(int i) const { return energies_.at(static_cast<size_t>(i)); }
   GpuSolver& instance(int i) { return *inst_.at(static_cast<size_t>(i)); }
   cudaStream_t stream() const { return stream_; }
@@ -52,6 +57,9 @@ class GpuBatch {
   void join_streams();
   void launch_iteration(Group& g);
   void build_graphs();
+  // The groups' launch descriptors over the active instances (instance i in
+  // group i % groups); drops the graphs.
+  void set_groups();
 
   SolverOptions opt_;
   std::vector<std::unique_ptr<GpuSolver>> inst_;
@@ -61,6 +69,7 @@ class GpuBatch {
   bool own_stream_ = false;
   long long graph_iters_ = 0;
   std::vector<double> energies_;
+  std::vector<char> active_;
 };
 
 }  // namespace mcd

@@ -83,3 +83,21 @@ def test_batch_callback_stops(batch_paths):
     seen = []
     b.solve(callback=lambda i, r: seen.append((i, r["iteration"])) or r["iteration"] >= 10000)
     assert seen == [(0, 5000), (1, 5000), (0, 10000), (1, 10000)]
+
+
+def test_batch_retires_instances(batch_paths):
+    """An instance retired by the callback (MCD_CB_RETIRE) stops advancing and
+    keeps its energy; the others run on without it, to the energies they
+    reach in the full batch, and the solve ends when none is left."""
+    b = m.CDFCIBatch([m.Fcidump(p) for p in batch_paths], **OPTS)
+    full = b.solve()
+    b.close()
+    b = m.CDFCIBatch([m.Fcidump(p) for p in batch_paths], **OPTS)
+    retire_at = {0: 5000, 2: 10000, 1: 15000, 3: 20000}
+    e = b.solve(callback=lambda i, r: "retire" if r["iteration"] >= retire_at[i] else False)
+    for i, reps in enumerate(b.reports):
+        assert [r["iteration"] for r in reps] == list(range(5000, retire_at[i] + 1, 5000)), i
+        assert e[i] == reps[-1]["energy"]
+    assert abs(e[3] - full[3]) < 1e-9
+    assert abs(e[1] - full[1]) < 1e-6
+    b.close()

@@ -205,6 +205,82 @@ def write_curve(d, points, seed):
     return paths
 
 
+CURVE_FIXTURE = os.path.join(HERE, "tests", "golden", "curve_energies.json")
+CURVE_TOL = 1e-6
+
+
+def curve_reference():
+    """Energies the reference reached on each curve point (its compiled solver
+    run by tests/golden/make_curve.py), or None when the fixture lacks points."""
+    try:
+        with open(CURVE_FIXTURE) as f:
+            data = json.load(f)
+    except OSError:
+        return None
+    pts = {p["point"]: p for p in data["points"]}
+    return pts if len(pts) == 32 else None
+
+
+def curve_time_to_reference(mc, paths, local_rank, ref, report=200, max_iterations=200000, sample=8):
+    """Wall time through the public API until every point's energy is within
+    1e-6 Ha of (at or below) the reference's energy on that point.  Batched:
+    mcd_batch_create + mcd_batch_solve, each instance retired at its first
+    report past its target, until the last gets there.  Plain: mcd_create +
+    mcd_solve point after point, each stopped at its first report past its
+    target, on `sample` evenly spaced points, summed and scaled to all of them.
+    Both include the set-up (Hamiltonian tables, tables, fills)."""
+    n = len(paths)
+    targets = [ref[i]["energy"] + CURVE_TOL for i in range(n)]
+    opts = dict(num_of_coordinate=CURVE_K, estimate=CURVE_K, max_memory=CURVE_GB, z_threshold=0.0,
+                threshold=0.0, device=local_rank, num_iterations=max_iterations, report_interval=report)
+    fc = [mc.Fcidump(p) for p in paths]
+    reached_b = {}
+    t0 = time.perf_counter()
+    b = mc.CDFCIBatch(fc, **opts)
+
+    def bcb(i, r):
+        if r["energy"] <= targets[i]:
+            reached_b[i] = (time.perf_counter() - t0, r["iteration"], r["energy"])
+            return "retire"
+        return False
+
+    b.solve(callback=bcb)
+    t_batch = time.perf_counter() - t0
+    b.close()
+    idx = sorted({round(j * (n - 1) / (sample - 1)) for j in range(sample)})
+    plain = []
+    for i in idx:
+        t1 = time.perf_counter()
+        s = mc.CDFCI(fc[i], **opts)
+        got = {}
+
+        def pcb(r, i=i, got=got):
+            if r["energy"] <= targets[i]:
+                got["it"] = r["iteration"]
+                return True
+            return False
+
+        s.solve(callback=pcb)
+        plain.append((i, time.perf_counter() - t1, got.get("it")))
+        s.close()
+    plain_s = sum(t for _, t, _ in plain) * n / len(plain)
+    ok_b = len(reached_b) == n
+    ok_p = all(it is not None for _, _, it in plain)
+    return {
+        "metric": "time to E within 1e-6 Ha of the reference, batched vs plain", "unit": "s",
+        "batched_s": t_batch if ok_b else None, "plain_s": plain_s if ok_p else None,
+        "speedup": (plain_s / t_batch) if (ok_b and ok_p) else None,
+        "points_reached_batched": len(reached_b),
+        "iterations_to_target_batched": {"min": min(v[1] for v in reached_b.values()) if reached_b else None,
+                                         "max": max(v[1] for v in reached_b.values()) if reached_b else None},
+        "plain_sample": [{"point": i, "seconds": t, "iterations": it} for i, t, it in plain],
+        "target": ("per point, the reference's energy + 1e-6 Ha, the reference (the solver compiled from its "
+                   "sources, tests/golden/make_curve.py) after " + str(ref[0]["iterations"]) + " iterations at k = "
+                   + str(ref[0]["k"]) + "; checked at reports every " + str(report) + " iterations"),
+        "plain_is": f"sum over {len(plain)} evenly spaced points of create + solve to the target, times {n}/{len(plain)}",
+    }
+
+
 def curve_throughput(mc, paths, local_rank, steps=500, warmup=500):
     """Device-timed coordinate updates/s: the whole curve as one batch, and
     one point on its own."""
@@ -539,7 +615,13 @@ def b200_arm(args, rank, world, local_rank):
         batched = None
         if not args.no_batched:
             ctmp = tempfile.mkdtemp(prefix="mcd_curve_", dir=tmp)
-            batched = curve_throughput(mc, write_curve(ctmp, args.curve_points, args.seed), local_rank)
+            cpaths = write_curve(ctmp, args.curve_points, args.seed)
+            batched = curve_throughput(mc, cpaths, local_rank)
+            ref = curve_reference()
+            if ref is not None and args.curve_points == 32:
+                batched["time_to_reference"] = curve_time_to_reference(mc, cpaths, local_rank, ref)
+            else:
+                batched["time_to_reference"] = {"unavailable": "tests/golden/curve_energies.json lacks points"}
 
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_EXE):

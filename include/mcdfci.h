@@ -115,6 +115,11 @@ typedef struct mcd_report {
   uint64_t updates_total; /* z updates since the last reset */
   uint64_t occupied;      /* occupied hash slots */
   int32_t last_k;         /* determinants picked in the last iteration */
+  int32_t inv_steps_last; /* inverse-iteration steps of the last eigenproblem (0: full reduction) */
+  uint64_t inv_updates;   /* eigenproblems solved by shifted inverse iteration since the reset */
+  uint64_t inv_steps;     /* their steps, summed */
+  uint64_t eig_fallbacks; /* shifted solves that fell back to the full reduction */
+  double max_abs_evec;    /* max |v_i|, i >= 1, of the last subspace eigenvector */
 } mcd_report;
 
 /* Called after every report_interval iterations; return nonzero to stop. */

@@ -88,7 +88,8 @@ class mcd_report(ctypes.Structure):
         ("updates", ctypes.c_uint64), ("time_s", ctypes.c_double), ("scale", ctypes.c_double),
         ("max_residual", ctypes.c_double), ("z_threshold", ctypes.c_double),
         ("emitted_total", ctypes.c_uint64), ("updates_total", ctypes.c_uint64), ("occupied", ctypes.c_uint64),
-        ("last_k", ctypes.c_int32),
+        ("last_k", ctypes.c_int32), ("inv_steps_last", ctypes.c_int32), ("inv_updates", ctypes.c_uint64),
+        ("inv_steps", ctypes.c_uint64), ("eig_fallbacks", ctypes.c_uint64), ("max_abs_evec", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

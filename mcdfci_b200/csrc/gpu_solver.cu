@@ -723,6 +723,11 @@ mcd_report GpuSolver::report() {
   r.occupied = 0;
   check(cudaMemcpy(&r.occupied, d_occ_, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "occupancy read");
   r.last_k = h_state_.k_cur;
+  r.inv_steps_last = h_state_.inv_steps_curr;
+  r.inv_updates = h_state_.inv_updates;
+  r.inv_steps = h_state_.inv_steps;
+  r.eig_fallbacks = h_state_.eig_fallbacks;
+  r.max_abs_evec = h_state_.max_abs_evec;
   occ_exact_ = r.occupied;
   occ_exact_iters_ = iters_enqueued_;
   setup_ms_[6] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1155,8 +1160,19 @@ int GpuSolver::solve(mcd_report_cb cb, void* user) {
         std::cout << std::setw(10) << std::fixed << std::setprecision(2) << r.time_s;
         std::cout << std::setw(10) << std::fixed << std::setprecision(6) << r.scale;
         std::cout << std::endl;
-        std::printf("[LOG] max residual: %e, subspace problem: %s\n", r.max_residual,
-                    h_state_.last_branch == 2 ? "k x k" : "(k+1) x (k+1)");
+        // The reference's fields (src/solver.h:787-798) with this solver's
+        // quantities: iterations solved by shifted inverse iteration, their
+        // steps, and the change made by the last refinement step; the
+        // updates that fell back to the full reduction are counted after.
+        const IterState& S = h_state_;
+        const double nit = S.inv_updates > 0 ? static_cast<double>(S.inv_updates) : 1.0;
+        std::printf(
+            "[LOG] max residual: %e, max eigenvector entry: %e, number of iterations provoking inv iters: %llu, "
+            "avg number of inv iters: %.1f, curr number of inv iters: %d, avg diff inv iter makes: %e, curr diff "
+            "inv iter makes: %e, max diff inv iter makes: %e, full reductions after a failed shift: %llu.\n",
+            r.max_residual, S.max_abs_evec, static_cast<unsigned long long>(S.inv_updates),
+            static_cast<double>(S.inv_steps) / nit, S.inv_steps_curr, S.inv_diff_sum / nit, S.inv_diff_curr,
+            S.inv_diff_max, static_cast<unsigned long long>(S.eig_fallbacks));
         std::fflush(stdout);
       }
       if (cb && cb(&r, user) != 0) {

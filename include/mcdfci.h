@@ -96,6 +96,13 @@ typedef struct mcd_options {
    * reserves its table.  A growth that finds the device memory taken by
    * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
   int32_t table_growth;
+  /* 1 (default): each subspace eigenproblem is first solved by shifted
+   * inverse iteration (a Cholesky factorisation of B - sigma I, sigma below
+   * the current energy by 16 times the last energy drop, certifies sigma <
+   * lambda_1; the current vector starts it), with the full reduction when
+   * that fails; 0: the full reduction every time.  No counterpart in the
+   * reference (LAPACK dsyevr, src/solver.h:400-411). */
+  int32_t eig_shift;
 } mcd_options;
 
 /* One line of the reference's report table (src/solver.h:761-798). */
@@ -311,12 +318,13 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
  * No counterpart in the reference. */
 int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
                            double* slots_per_s);
-/* SM cycles spent in each phase of the leader kernel (17 phases: state load,
+/* SM cycles spent in each phase of the leader kernel (21 phases: state load,
  * finish, candidate gather, top-k, tie sort, picked, H_sub, update_x, publish,
  * eig setup, tridiagonalisation, multisection, inverse iteration,
  * back-transformation, Rayleigh quotient, eig finish, shifted inverse
- * iteration), summed over launches since the previous call, which resets
- * them.  No counterpart in the reference. */
+ * iteration set-up, its Cholesky factorisation, explicit inverse, power steps
+ * and refinement steps), summed over launches since the previous call, which
+ * resets them.  No counterpart in the reference. */
 int mcd_debug_leader_sections(mcd_solver* s, uint64_t* cycles, int32_t n);
 /* The determinants with nonzero x and their x (the coefficients are scale * x),
  * sorted by slot; up to cap of them, *n_out receives the count. */

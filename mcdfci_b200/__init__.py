@@ -77,7 +77,7 @@ class mcd_options(ctypes.Structure):
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
-        ("table_growth", ctypes.c_int32),
+        ("table_growth", ctypes.c_int32), ("eig_shift", ctypes.c_int32),
     ]
 
 
@@ -287,7 +287,7 @@ def make_options(**kw) -> mcd_options:
     """mcd_options with the reference defaults, then keyword overrides
     (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
     z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
-    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth)."""
+    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth, eig_shift)."""
     o = mcd_options()
     library().mcd_options_default(ctypes.byref(o))
     occ = kw.pop("ref_det_occ", None)
@@ -299,7 +299,7 @@ def make_options(**kw) -> mcd_options:
             o.stream = ctypes.c_void_p(int(v) if v else 0)
         elif k == "z_threshold_search":
             o.z_threshold_search = int(bool(v))
-        elif k in ("compaction", "table_growth"):
+        elif k in ("compaction", "table_growth", "eig_shift"):
             setattr(o, k, int(bool(v)))
         else:
             setattr(o, k, v)
@@ -514,7 +514,8 @@ class CDFCI:
 
     LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
-                       "rayleigh", "eig_finish", "shifted")
+                       "rayleigh", "eig_finish", "shifted", "shift_cholesky", "shift_inverse", "shift_power",
+                       "shift_refine")
 
     def leader_sections(self) -> dict:
         """SM cycles per leader-kernel phase since the previous call."""

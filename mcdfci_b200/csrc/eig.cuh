@@ -798,7 +798,7 @@ __device__ __forceinline__ double shift_sum(double v, double* part, int nw, int 
 }
 
 __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
-                                   int* steps, double* diff) {
+                                   int* steps, double* diff, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = (n + 31) >> 5;  // warps with a row each
   __shared__ bool s_ok;
@@ -857,6 +857,7 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
     if (lane == 0 && !ok) s_ok = false;
   }
   __syncthreads();
+  clk.mark(17);
   if (!s_ok) {
     *steps = 0;
     *diff = 0.0;
@@ -881,6 +882,7 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
     }
   }
   __syncthreads();
+  clk.mark(18);
 
   // (c) Power steps on C = L^-T L^-1 by the first nw warps; the others wait
   //     at the closing barrier.  v in V.y (normalised first), L^-1 v in V.c.
@@ -917,6 +919,7 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
       conv = dv < 1e-12 || (dv < 1e-8 && dv > 0.5 * prev);
       prev = dv;
     }
+    clk.mark(19);
     // (d) Refinement steps: w = v - C r, r = A v - rho v.
     bool done = false;
     for (int it = 0; it < kShiftRefineSteps && !done; ++it) {
@@ -957,6 +960,7 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
     }
   }
   __syncthreads();
+  clk.mark(20);
   *steps = s_steps;
   *diff = s_diff;
   return s_ok;

@@ -34,6 +34,9 @@ struct SolverOptions {
   // allocation) as it fills, up to the size max_memory gives; false: the
   // whole table is allocated at creation, as the reference reserves it.
   bool table_growth = true;
+  // Subspace eigenproblem: shifted inverse iteration first (falling back to
+  // the full reduction), or the full reduction every time.
+  bool eig_shift = true;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;

@@ -103,6 +103,7 @@ struct LeaderLaunch {
   unsigned long long* sect;  // [kLeaderSections] SM cycles per phase of the leader kernel, or null
   int m;
   int k_req;
+  int eig_shift;          // 1: shifted inverse iteration first when the last energy drop is known
 };
 
 // Several independent instances advanced by the same two launches per
@@ -147,8 +148,10 @@ struct RdmLaunch {
 // 7 update_x, 8 publish, 9 eig setup, 10 tridiagonalisation, 11 multisection,
 // 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
 // 15 eig finish,
-// 16 shifted inverse iteration (when it runs, in place of 10-13).
-constexpr int kLeaderSections = 17;
+// 16 shifted inverse iteration (when it runs, in place of 10-13: its set-up
+// and, when it fails, the restore), split into 17 Cholesky factorisation,
+// 18 explicit inverse, 19 power steps, 20 refinement steps.
+constexpr int kLeaderSections = 21;
 
 // Phases of the column kernel timed into ColumnLaunch::sect (thread 0 of each
 // CTA, summed): 0 entry decode and integral value, 1 slot probe, 2 x load,

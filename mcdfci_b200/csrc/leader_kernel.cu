@@ -285,7 +285,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     __syncthreads();
     int steps = 0;
     double diff = 0.0;
-    shifted = eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff);
+    shifted = eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff, clk);
     res.shift_steps = shifted ? steps : 0;
     res.shift_diff = shifted ? diff : 0.0;
     if (!shifted) {
@@ -848,7 +848,7 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
     for (int t = tid; t < k * k; t += kLT) L.hsub_out[t] = Hs[t];
 
   // 6. Eig update.
-  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, sS.eig_drop);
+  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0);
   clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {

@@ -430,6 +430,48 @@ def phases_arm(args, local_rank):
     return 0
 
 
+def curve_sharded_arm(args, rank, world, local_rank):
+    """The curve spread over the node's GPUs (mcdfci_b200.curve): point i on
+    rank i mod world, each rank's share solved as one batch, energies gathered
+    to rank 0; wall time from a barrier before the first creation to a
+    barrier after the last solve, max over ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from mcdfci_b200 import curve
+    from mcdfci_b200.replicas import max_over_ranks
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    tmp = tempfile.mkdtemp(prefix="mcd_curve_")
+    try:
+        paths = write_curve(tmp, args.curve_points, args.seed)
+        opts = dict(num_of_coordinate=CURVE_K, estimate=CURVE_K, max_memory=CURVE_GB, z_threshold=0.0,
+                    threshold=0.0, device=local_rank, num_iterations=args.curve_iterations,
+                    report_interval=args.curve_report)
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = curve.solve_curve(len(paths), curve.batch_solver(paths, **opts), dist)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        wall = max_over_ranks(dt, dist, "cuda")
+        if rank == 0:
+            print(json.dumps({
+                "metric": "curve wall time, points spread over GPUs", "unit": "s", "value": wall,
+                "higher_is_better": False, "n_gpus": world, "scaling": "strong",
+                "points": len(paths), "energies": [r["energy"] for r in out],
+                "config": {"workload": f"{len(paths)} x {CURVE} points (t = 0..1), k = m = {CURVE_K}, "
+                                       f"{CURVE_GB} GB table each", "iterations": args.curve_iterations,
+                           "report_interval": args.curve_report, "sharding": "point i on rank i mod world"},
+                "dtype": "f64", "data": "synthetic (mcdfci_b200.synth)"}))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        dist.destroy_process_group()
+    return 0
+
+
 def write_workload(d, seed):
     from mcdfci_b200 import synth
 
@@ -726,11 +768,11 @@ def main():
         torch.cuda.set_device(local_rank)
         return phases_arm(args, local_rank)
     if args.workload == "curve":
-        if world > 1 and rank != 0:
-            return 0
         import torch
 
         torch.cuda.set_device(local_rank)
+        if world > 1:
+            return curve_sharded_arm(args, rank, world, local_rank)
         return curve_arm(args, local_rank)
     if world > 1:
         import datetime

@@ -92,8 +92,8 @@ def parse_args():
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
     ap.add_argument("--phase-workload", default="n24_6a6b")
-    ap.add_argument("--no-eig-shift", action="store_true",
-                    help="solve every subspace eigenproblem by the full reduction")
+    ap.add_argument("--eig-shift", type=int, default=2, choices=[0, 1, 2],
+                    help="subspace eigenproblem: 2 shifted (one-warp steps), 1 shifted (block steps), 0 full reduction")
     ap.add_argument("--scatter-sweep", action="store_true",
                     help="with --phases: also sweep the table's scattered-access probe")
     return ap.parse_args()
@@ -386,7 +386,7 @@ def phases_arm(args, local_rank):
         synth.write_fcidump(path, args.phase_workload, seed=args.seed)
         s = mc.CDFCI(mc.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                      z_threshold=args.z_threshold, threshold=0.0, groups=args.groups, device=local_rank,
-                     eig_shift=not args.no_eig_shift)
+                     eig_shift=args.eig_shift)
         s.reset()
         s.run_iterations(args.warmup)
         rb = s.report()
@@ -424,7 +424,7 @@ def phases_arm(args, local_rank):
         "column_cycles_per_round": {k: round(v / rounds) for k, v in col.items()},
         "column_cycles_per_cta": per_cta,
         "column_rounds_per_cta": round(rounds / ctas, 2),
-        "energy": rep["energy"], "z_size": rep["z_size"], "eig": eig, "eig_shift": not args.no_eig_shift,
+        "energy": rep["energy"], "z_size": rep["z_size"], "eig": eig, "eig_shift": args.eig_shift,
         "scatter_probe": scatter,
     }, indent=1))
     return 0

@@ -299,7 +299,9 @@ def make_options(**kw) -> mcd_options:
             o.stream = ctypes.c_void_p(int(v) if v else 0)
         elif k == "z_threshold_search":
             o.z_threshold_search = int(bool(v))
-        elif k in ("compaction", "table_growth", "eig_shift"):
+        elif k == "eig_shift":
+            o.eig_shift = int(v)
+        elif k in ("compaction", "table_growth"):
             setattr(o, k, int(bool(v)))
         else:
             setattr(o, k, v)

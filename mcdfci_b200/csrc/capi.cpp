@@ -72,7 +72,8 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.groups = o->groups;
   s.compaction = o->compaction != 0;
   s.table_growth = o->table_growth != 0;
-  s.eig_shift = o->eig_shift != 0;
+  if (o->eig_shift < 0 || o->eig_shift > 2) throw mcd::McdError(MCD_ERR_INVALID, "eig_shift must be 0, 1 or 2.");
+  s.eig_shift = o->eig_shift;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -157,7 +158,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   if (cd.has("groups")) o->groups = static_cast<int32_t>(cd.at("groups").as_number("groups"));
   if (cd.has("compaction")) o->compaction = cd.at("compaction").as_bool("compaction") ? 1 : 0;
   if (cd.has("table_growth")) o->table_growth = cd.at("table_growth").as_bool("table_growth") ? 1 : 0;
-  if (cd.has("eig_shift")) o->eig_shift = cd.at("eig_shift").as_bool("eig_shift") ? 1 : 0;
+  if (cd.has("eig_shift")) o->eig_shift = static_cast<int32_t>(cd.at("eig_shift").as_number("eig_shift"));
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -194,7 +195,7 @@ void mcd_options_default(mcd_options* o) {
   o->groups = 0;
   o->compaction = 0;
   o->table_growth = 1;
-  o->eig_shift = 1;
+  o->eig_shift = 2;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;

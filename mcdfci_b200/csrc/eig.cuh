@@ -966,4 +966,242 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
   return s_ok;
 }
 
+// The same method with (c) and (d) run by one warp on the explicit
+// C = L^-T L^-1 (formed once by the whole block into Ci): each power step
+// is one matrix-vector product with up to kShiftQ rows per lane and two
+// shuffle reductions, with no block barrier; each refinement step adds the
+// residual's product with A (upper triangle and V.d).  (a) and (b) as in
+// eig_lowest_shifted.  Same contract, plus Ci: n x lda shared doubles.
+__device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
+                                        double* Ci, int* steps, double* diff, SectionClock& clk) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ bool s_ok;
+  __shared__ int s_steps;
+  __shared__ double s_diff;
+  if (tid == 0) {
+    s_ok = true;
+    s_steps = 0;
+    s_diff = 0.0;
+  }
+  for (int i = tid; i < n; i += blockDim.x) V.d[i] = A[i * lda + i];
+  __syncthreads();
+
+  // (a) Cholesky by warp 0.
+  if (warp == 0) {
+    bool ok = true;
+    for (int j = 0; j < n; ++j) {
+      const double* Lj = A + j * lda;
+      double sv[kShiftQ];
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = j + lane + 32 * q;
+        sv[q] = 0.0;
+        if (i < n) {
+          const double* Lr = A + i * lda;
+          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+          int c = 0;
+          for (; c + 4 <= j; c += 4) {
+            a0 = fma(Lr[c], Lj[c], a0);
+            a1 = fma(Lr[c + 1], Lj[c + 1], a1);
+            a2 = fma(Lr[c + 2], Lj[c + 2], a2);
+            a3 = fma(Lr[c + 3], Lj[c + 3], a3);
+          }
+          for (; c < j; ++c) a0 = fma(Lr[c], Lj[c], a0);
+          const double aij = (i == j) ? Lr[j] - sigma : Lr[j];
+          sv[q] = aij - ((a0 + a1) + (a2 + a3));
+        }
+      }
+      const double d = __shfl_sync(~0u, sv[0], 0);
+      if (!(d > 0.0)) {
+        ok = false;
+        break;
+      }
+      const double r = rsqrt(d);
+      if (lane == 0) {
+        A[j * lda + j] = d * r;
+        V.ru[j] = r;
+      }
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = j + lane + 32 * q;
+        if (i > j && i < n) A[i * lda + j] = sv[q] * r;
+      }
+      __syncwarp();
+    }
+    if (lane == 0 && !ok) s_ok = false;
+  }
+  __syncthreads();
+  clk.mark(17);
+  if (!s_ok) {
+    *steps = 0;
+    *diff = 0.0;
+    return false;
+  }
+
+  // (b) L^-1, column j by thread j.
+  if (tid < n) {
+    const int j = tid;
+    for (int i = 0; i < n; ++i) {
+      const double* Lr = A + i * lda;
+      double a0 = (i == j) ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int c = 0;
+      for (; c + 4 <= i; c += 4) {
+        a0 = fma(-Lr[c], Li[c * lda + j], a0);
+        a1 = fma(-Lr[c + 1], Li[(c + 1) * lda + j], a1);
+        a2 = fma(-Lr[c + 2], Li[(c + 2) * lda + j], a2);
+        a3 = fma(-Lr[c + 3], Li[(c + 3) * lda + j], a3);
+      }
+      for (; c < i; ++c) a0 = fma(-Lr[c], Li[c * lda + j], a0);
+      Li[i * lda + j] = ((a0 + a1) + (a2 + a3)) * V.ru[i];
+    }
+  }
+  __syncthreads();
+  // C = L^-T L^-1: C[i][j] = sum over c >= max(i, j) of Li[c][i] Li[c][j], one
+  // element of the upper triangle per thread, mirrored.
+  for (int t = tid; t < n * (n + 1) / 2; t += blockDim.x) {
+    int j = static_cast<int>((sqrtf(8.0f * static_cast<float>(t) + 1.0f) - 1.0f) * 0.5f);
+    while (j * (j + 1) / 2 > t) --j;
+    while ((j + 1) * (j + 2) / 2 <= t) ++j;
+    const int i = t - j * (j + 1) / 2;  // i <= j
+    double a0 = 0.0, a1 = 0.0;
+    int c = j;
+    for (; c + 2 <= n; c += 2) {
+      a0 = fma(Li[c * lda + i], Li[c * lda + j], a0);
+      a1 = fma(Li[(c + 1) * lda + i], Li[(c + 1) * lda + j], a1);
+    }
+    if (c < n) a0 = fma(Li[c * lda + i], Li[c * lda + j], a0);
+    const double v = a0 + a1;
+    Ci[i * lda + j] = v;
+    Ci[j * lda + i] = v;
+  }
+  __syncthreads();
+  clk.mark(18);
+
+  // (c), (d) by warp 0; rows lane + 32 q.
+  if (warp == 0) {
+    double v[kShiftQ];
+    double nrm = 0.0;
+#pragma unroll
+    for (int q = 0; q < kShiftQ; ++q) {
+      const int i = lane + 32 * q;
+      v[q] = i < n ? V.y[i] : 0.0;
+      nrm = fma(v[q], v[q], nrm);
+    }
+    nrm = warp_sum(nrm);
+    const double inv0 = rsqrt(nrm);
+#pragma unroll
+    for (int q = 0; q < kShiftQ; ++q) {
+      v[q] *= inv0;
+      const int i = lane + 32 * q;
+      if (i < n) V.y[i] = v[q];
+    }
+    __syncwarp();
+    // w = M u for the rows of this lane, u in shared memory.
+    auto matvec = [&](const double* M, const double* u, double (&w)[kShiftQ]) {
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = lane + 32 * q;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        if (i < n) {
+          const double* row = M + i * lda;
+          int c = 0;
+          for (; c + 4 <= n; c += 4) {
+            a0 = fma(row[c], u[c], a0);
+            a1 = fma(row[c + 1], u[c + 1], a1);
+            a2 = fma(row[c + 2], u[c + 2], a2);
+            a3 = fma(row[c + 3], u[c + 3], a3);
+          }
+          for (; c < n; ++c) a0 = fma(row[c], u[c], a0);
+        }
+        w[q] = (a0 + a1) + (a2 + a3);
+      }
+    };
+    // v <- w / |w|; returns |v_new - v_old|.
+    auto normalise_into = [&](double (&w)[kShiftQ]) {
+      double ww = 0.0;
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) ww = fma(w[q], w[q], ww);
+      ww = warp_sum(ww);
+      const double inv = rsqrt(ww);
+      double d2 = 0.0;
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const double vn = w[q] * inv;
+        d2 = fma(vn - v[q], vn - v[q], d2);
+        v[q] = vn;
+      }
+      d2 = warp_sum(d2);
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = lane + 32 * q;
+        if (i < n) V.y[i] = v[q];
+      }
+      __syncwarp();
+      return sqrt(d2);
+    };
+    int nsteps = 0;
+    double prev = 1e300;
+    for (int it = 0; it < kShiftPowerSteps; ++it) {
+      double w[kShiftQ];
+      matvec(Ci, V.y, w);
+      const double dv = normalise_into(w);
+      ++nsteps;
+      if (dv < 1e-12 || (dv < 1e-8 && dv > 0.5 * prev)) break;
+      prev = dv;
+    }
+    clk.mark(19);
+    bool done = false;
+    double last = 0.0;
+    for (int it = 0; it < kShiftRefineSteps && !done; ++it) {
+      // A v from the upper triangle and the saved diagonal.
+      double av[kShiftQ];
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = lane + 32 * q;
+        double a0 = 0.0, a1 = 0.0;
+        if (i < n) {
+          for (int c = 0; c < n; c += 2) {
+            const double e0 = (c == i) ? V.d[i] : (c > i ? A[i * lda + c] : A[c * lda + i]);
+            a0 = fma(e0, V.y[c], a0);
+            if (c + 1 < n) {
+              const int c1 = c + 1;
+              const double e1 = (c1 == i) ? V.d[i] : (c1 > i ? A[i * lda + c1] : A[c1 * lda + i]);
+              a1 = fma(e1, V.y[c1], a1);
+            }
+          }
+        }
+        av[q] = a0 + a1;
+      }
+      double rho = 0.0;
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) rho = fma(v[q], av[q], rho);
+      rho = warp_sum(rho);
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) {
+        const int i = lane + 32 * q;
+        if (i < n) V.g[i] = av[q] - rho * v[q];
+      }
+      __syncwarp();
+      double t[kShiftQ];
+      matvec(Ci, V.g, t);
+#pragma unroll
+      for (int q = 0; q < kShiftQ; ++q) t[q] = v[q] - t[q];
+      last = normalise_into(t);
+      ++nsteps;
+      done = last < 2e-15 * sqrt(static_cast<double>(n));
+    }
+    if (lane == 0) {
+      s_ok = done;
+      s_steps = nsteps;
+      s_diff = last;
+    }
+  }
+  __syncthreads();
+  clk.mark(20);
+  *steps = s_steps;
+  *diff = s_diff;
+  return s_ok;
+}
+
 }  // namespace mcd

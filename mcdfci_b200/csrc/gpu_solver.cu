@@ -435,7 +435,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.sect = d_sect_;
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
-  ll_.eig_shift = opt_.eig_shift ? 1 : 0;
+  ll_.eig_shift = opt_.eig_shift;
   const auto t_up = clock::now();
   check(cudaStreamSynchronize(stream_), "table upload");
   upload_ms = ms_since(t_up);

@@ -166,10 +166,11 @@ struct EigResult {
 constexpr int kEigVecs = 18;
 
 // Shared scratch of eig_update: B (lda), 18 vectors, and for k + 1 <=
-// kShiftMaxN the explicit inverse of the shifted solver's Cholesky factor.
+// kShiftMaxN the explicit inverse of the shifted solver's Cholesky factor
+// and the inverse of B - sigma I formed from it.
 __host__ __device__ constexpr size_t eig_work_doubles(int k) {
   return static_cast<size_t>(k + 1) * eig_lda(k + 1) + kEigVecs * static_cast<size_t>(k + 1) +
-         (k + 1 <= kShiftMaxN ? static_cast<size_t>(k + 1) * eig_lda(k + 1) : 0) + 64;
+         (k + 1 <= kShiftMaxN ? 2 * static_cast<size_t>(k + 1) * eig_lda(k + 1) : 0) + 64;
 }
 
 // drop: the last update's energy drop E - lambda (0 = unknown).  When it is
@@ -179,8 +180,10 @@ __host__ __device__ constexpr size_t eig_work_doubles(int k) {
 // its Rayleigh quotient there is xz/xx) and the current vector as the start;
 // the reduction runs when that fails or its residual is not below 1e-11
 // (1 + |lambda|).
+// method: 1 the block-wide steps (eig_lowest_shifted), 2 the one-warp steps
+// on the explicit inverse (eig_lowest_shifted_warp).
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
-                                double* dx, double* work, SectionClock& clk, double drop) {
+                                double* dx, double* work, SectionClock& clk, double drop, int method = 2) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1, s_res;
   __shared__ int s_branch;
@@ -215,7 +218,8 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   double* vhi = vec + 15 * vs;   // normalised eigenvector, hi part
   double* vlo = vec + 16 * vs;   // lo part
 
-  double* Li = vec + kEigVecs * vs;  // [(k+1) x lda] when k + 1 <= kShiftMaxN
+  double* Li = vec + kEigVecs * vs;   // [(k+1) x lda] when k + 1 <= kShiftMaxN
+  double* Ci = Li + vs * lda;          // [(k+1) x lda] likewise
   auto fill_h = [&]() {
     for (int idx = tid; idx < k * k; idx += blockDim.x) {
       const int i = idx / k, j = idx - i * k;
@@ -285,7 +289,8 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     __syncthreads();
     int steps = 0;
     double diff = 0.0;
-    shifted = eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff, clk);
+    shifted = method == 1 ? eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff, clk)
+                          : eig_lowest_shifted_warp(A, lda, n, V, e_cur - delta, Li, Ci, &steps, &diff, clk);
     res.shift_steps = shifted ? steps : 0;
     res.shift_diff = shifted ? diff : 0.0;
     if (!shifted) {
@@ -848,7 +853,8 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
     for (int t = tid; t < k * k; t += kLT) L.hsub_out[t] = Hs[t];
 
   // 6. Eig update.
-  const EigResult er = eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0);
+  const EigResult er =
+      eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0, L.eig_shift);
   clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {

@@ -8,7 +8,9 @@ computes:
 - with k = 1 (one column per iteration, so no two adds race on a slot) a solve
   that grows reports the same energies, sizes and counters as one that holds
   the whole table from the start;
-- after growths, the solver's xx and xz still equal the sums over the table
+- after growths (k = 1 on the 16-orbital workload: a first table of 2^20
+  slots that grows within 3000 iterations), the solver's xx and xz still
+  equal the sums over the table
   (WaveFunctionCuckoo::debug_calculate_xx_xz, src/wavefunction.h:640-667);
 - a checkpoint with more entries than a fresh solver's first table loads into
   it (the table grows first) and continues the solve.
@@ -49,11 +51,11 @@ def test_growth_gives_the_same_solve_k1(synth_fcidumps):
 
 def test_scalars_match_table_after_growth(synth_fcidumps):
     path = synth_fcidumps["n16_5a5b"]
-    s = m.CDFCI(m.Fcidump(path), num_of_coordinate=16, estimate=16, max_memory=1.0, threshold=0.0,
+    s = m.CDFCI(m.Fcidump(path), num_of_coordinate=1, estimate=16, max_memory=1.0, threshold=0.0,
                 z_threshold=0.0)
     s.reset()
     cap0 = s.table_info()["capacity"]
-    s.run_iterations(2500)
+    s.run_iterations(3000)
     info = s.table_info()
     assert info["growths"] >= 1 and info["capacity"] > cap0
     sc = s.scalars()
@@ -70,10 +72,10 @@ def test_scalars_match_table_after_growth(synth_fcidumps):
 def test_checkpoint_loads_into_a_smaller_first_table(synth_fcidumps, tmp_path):
     path = synth_fcidumps["n16_5a5b"]
     ck = os.path.join(str(tmp_path), "n16.ckpt")
-    kw = dict(num_of_coordinate=16, estimate=16, max_memory=1.0, threshold=0.0, z_threshold=0.0)
+    kw = dict(num_of_coordinate=1, estimate=16, max_memory=1.0, threshold=0.0, z_threshold=0.0)
     a = m.CDFCI(m.Fcidump(path), **kw)
     a.reset()
-    a.run_iterations(2500)
+    a.run_iterations(3000)
     r_mid = a.report()
     a.save(ck)
     a.run_iterations(200)
@@ -90,5 +92,5 @@ def test_checkpoint_loads_into_a_smaller_first_table(synth_fcidumps, tmp_path):
     b.run_iterations(200)
     r_b = b.report()
     assert r_b["iteration"] == r_a["iteration"]
-    assert abs(r_b["energy"] - r_a["energy"]) < 1e-7
+    assert abs(r_b["energy"] - r_a["energy"]) < 1e-9
     b.close()

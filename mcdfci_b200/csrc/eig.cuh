@@ -966,6 +966,99 @@ __device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, 
   return s_ok;
 }
 
+// (a) and (b) with the matrix in registers, for n <= kShiftRegRows: 160
+// threads, row r = t/4 held by four lanes, lane quarter q keeping columns
+// 9q..9q+8.  Cholesky, right-looking: at step j the owners of column j
+// publish it (rows >= j) to a shared vector, and after one barrier every
+// thread scales it by 1/sqrt(pivot) and updates its part of the trailing
+// matrix; L goes to A's lower triangle, 1/L_jj to V.ru.  Then X = L^-1 by
+// forward substitution on the identity, row j published (divided by L_jj)
+// and subtracted from the rows below, one barrier per step; X goes to Li.
+// Two vectors alternate as the published column or row, so that a step's
+// writes never meet the previous step's reads.  Called by the whole block;
+// returns false (uniform) on a non-positive pivot.
+constexpr int kShiftRegRows = 36;
+constexpr int kShiftRegThreads = 160;
+
+__device__ bool shift_factor_reg(double* A, int lda, int n, double sigma, const EigVecs& V, double* Li) {
+  const int t = threadIdx.x;
+  const bool part = t < kShiftRegThreads;
+  const int r = t >> 2, q = t & 3;
+  const bool row_ok = part && r < n;
+  __shared__ int s_fail;
+  double a[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) {
+    const int c = 9 * q + e;
+    a[e] = (row_ok && c < n) ? A[r * lda + c] - (r == c ? sigma : 0.0) : 0.0;
+  }
+  if (t == 0) s_fail = 0;
+  __syncthreads();
+  if (part) {
+    for (int j = 0; j < n; ++j) {
+      double* col = (j & 1) ? V.g : V.c;
+      if (row_ok && r >= j && q == j / 9) col[r] = reg_pick9(a, j - 9 * q);
+      bar_named(2, kShiftRegThreads);
+      const double d = col[j];
+      if (!(d > 0.0)) {
+        if (t == 0) s_fail = 1;
+        break;
+      }
+      const double rinv = rsqrt(d);
+      if (row_ok && r > j) {
+        const double li = col[r] * rinv;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          const int c = 9 * q + e;
+          if (c > j && c < n) a[e] = fma(-li, col[c] * rinv, a[e]);
+        }
+        if (q == 0) A[r * lda + j] = li;
+      }
+      if (r == j && q == 0) {
+        A[j * lda + j] = d * rinv;
+        V.ru[j] = rinv;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_fail) return false;
+  if (part) {
+    double x[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) x[e] = (row_ok && r == 9 * q + e) ? 1.0 : 0.0;
+    for (int j = 0; j < n; ++j) {
+      double* row = (j & 1) ? V.den : V.num;
+      if (r == j) {
+        const double rinv = V.ru[j];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          const int c = 9 * q + e;
+          x[e] *= rinv;
+          if (c < n) row[c] = x[e];
+        }
+      }
+      bar_named(2, kShiftRegThreads);
+      if (row_ok && r > j) {
+        const double lij = A[r * lda + j];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          const int c = 9 * q + e;
+          if (c <= j) x[e] = fma(-lij, row[c], x[e]);
+        }
+      }
+    }
+    if (row_ok) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        const int c = 9 * q + e;
+        if (c < n) Li[r * lda + c] = x[e];
+      }
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
 // The same method with (c) and (d) run by one warp on the explicit
 // C = L^-T L^-1 (formed once by the whole block into Ci): each power step
 // is one matrix-vector product with up to kShiftQ rows per lane and two
@@ -986,6 +1079,15 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
   for (int i = tid; i < n; i += blockDim.x) V.d[i] = A[i * lda + i];
   __syncthreads();
 
+  if (n <= kShiftRegRows) {
+    const bool ok = shift_factor_reg(A, lda, n, sigma, V, Li);
+    clk.mark(17);
+    if (!ok) {
+      *steps = 0;
+      *diff = 0.0;
+      return false;
+    }
+  } else {
   // (a) Cholesky by warp 0.
   if (warp == 0) {
     bool ok = true;
@@ -1056,6 +1158,7 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
     }
   }
   __syncthreads();
+  }
   // C = L^-T L^-1: C[i][j] = sum over c >= max(i, j) of Li[c][i] Li[c][j], one
   // element of the upper triangle per thread, mirrored.
   for (int t = tid; t < n * (n + 1) / 2; t += blockDim.x) {

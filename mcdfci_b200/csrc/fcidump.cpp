@@ -98,6 +98,7 @@ Fcidump read_fcidump(const std::string& path) {
     d.nelec = read_int_param(header, "NELEC");
     d.ms2 = read_int_param(header, "MS2");
     d.uhf = read_uhf_param(header);
+    d.spin_conserving = !d.uhf;  // rhf_insert writes alpha-alpha and beta-beta pairs only
     const int nfile = d.norb;  // largest index allowed in the body
     if (!d.uhf) d.norb *= 2;
     if (d.norb <= 0 || d.norb > 2 * kMaxOrb)

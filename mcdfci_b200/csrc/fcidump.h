@@ -19,6 +19,9 @@ struct Fcidump {
   int nelec = 0;
   int ms2 = 0;
   bool uhf = false;
+  // True when every integral conserves spin by construction (the RHF
+  // expansion of a file), so that the tables need not check it.
+  bool spin_conserving = false;
   double core_energy = 0.0;
   std::vector<double> h1;       // [norb*norb] <i|h|a>
   // <ij|ab> stored densely at ((i*norb+j)*norb+a)*norb+b for i <= j, the only

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <iomanip>
 #include <iostream>
+#include <mutex>
 #include <sstream>
 
 namespace mcd {
@@ -237,6 +238,32 @@ T* device_alloc(size_t count, const char* what) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Pinned host words for the occupancy reads, two per solver, from blocks
+// that stay allocated for the life of the process (page-locking a fresh
+// block costs more than a solver's other set-up), reused as solvers go.
+std::mutex g_pin_mu;
+std::vector<unsigned long long*> g_pin_free;
+
+unsigned long long* pinned_words_acquire() {
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  if (g_pin_free.empty()) {
+    constexpr int kPairs = 256;
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocHost(&p, kPairs * 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) throw McdError(MCD_ERR_CUDA, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+    auto* b = static_cast<unsigned long long*>(p);
+    for (int i = kPairs - 1; i >= 0; --i) g_pin_free.push_back(b + 2 * i);
+  }
+  unsigned long long* w = g_pin_free.back();
+  g_pin_free.pop_back();
+  return w;
+}
+
+void pinned_words_release(unsigned long long* w) {
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pin_free.push_back(w);
+}
+
 }  // namespace
 
 void GpuSolver::check(cudaError_t e, const char* what) {
@@ -383,22 +410,38 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     hd_.wab = reinterpret_cast<const double*>(base + o_wab);
 
     d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
-    d_state_ = device_alloc<IterState>(1, "iteration state");
-    d_cand_score_ = device_alloc<double>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
-    d_cand_slot_ = device_alloc<unsigned>(static_cast<size_t>(kMaxK) * opt_.m, "candidates");
-    d_hsub_ = device_alloc<double>(static_cast<size_t>(kMaxK) * kMaxK, "H_sub");
-    d_err_ = device_alloc<unsigned>(1, "error word");
-    d_occ_ = device_alloc<unsigned long long>(1, "occupancy");
-    d_sect_ = device_alloc<unsigned long long>(kLeaderSections + kColumnSections, "phase timers");
+    // The iteration's small buffers in one allocation.
+    const size_t parts = static_cast<size_t>(opt_.k) * groups_;
+    const size_t mk = static_cast<size_t>(kMaxK) * opt_.m;
+    size_t mo = 0;
+    auto carve = [&](size_t bytes) {
+      const size_t o = mo;
+      mo = align_up(mo + bytes, 256);
+      return o;
+    };
+    const size_t o_state = carve(sizeof(IterState)), o_cs = carve(mk * sizeof(double)),
+                 o_cl = carve(mk * sizeof(unsigned)), o_h = carve(static_cast<size_t>(kMaxK) * kMaxK * sizeof(double)),
+                 o_err = carve(sizeof(unsigned)), o_occ = carve(sizeof(unsigned long long)),
+                 o_sect = carve((kLeaderSections + kColumnSections) * sizeof(unsigned long long)),
+                 o_pk = carve(parts * list_ * sizeof(unsigned long long)), o_ps = carve(parts * list_ * sizeof(unsigned)),
+                 o_psum = carve(parts * kPartSum * sizeof(double)), o_done = carve(kMaxK * sizeof(unsigned));
+    d_misc_ = device_alloc<unsigned char>(mo, "iteration buffers");
+    unsigned char* mb = static_cast<unsigned char*>(d_misc_);
+    d_state_ = reinterpret_cast<IterState*>(mb + o_state);
+    d_cand_score_ = reinterpret_cast<double*>(mb + o_cs);
+    d_cand_slot_ = reinterpret_cast<unsigned*>(mb + o_cl);
+    d_hsub_ = reinterpret_cast<double*>(mb + o_h);
+    d_err_ = reinterpret_cast<unsigned*>(mb + o_err);
+    d_occ_ = reinterpret_cast<unsigned long long*>(mb + o_occ);
+    d_sect_ = reinterpret_cast<unsigned long long*>(mb + o_sect);
+    d_part_key_ = reinterpret_cast<unsigned long long*>(mb + o_pk);
+    d_part_slot_ = reinterpret_cast<unsigned*>(mb + o_ps);
+    d_part_sum_ = reinterpret_cast<double*>(mb + o_psum);
+    d_done_ = reinterpret_cast<unsigned*>(mb + o_done);
     check(cudaMemsetAsync(d_sect_, 0, (kLeaderSections + kColumnSections) * sizeof(unsigned long long), stream_),
           "memset");
-    const size_t parts = static_cast<size_t>(opt_.k) * groups_;
-    d_part_key_ = device_alloc<unsigned long long>(parts * list_, "column partial lists");
-    d_part_slot_ = device_alloc<unsigned>(parts * list_, "column partial lists");
-    d_part_sum_ = device_alloc<double>(parts * kPartSum, "column partial sums");
-    d_done_ = device_alloc<unsigned>(kMaxK, "column tickets");
     check(cudaMemsetAsync(d_done_, 0, kMaxK * sizeof(unsigned), stream_), "memset");
-    check(cudaMallocHost(&h_occ_, 2 * sizeof(unsigned long long)), "cudaMallocHost");
+    h_occ_ = pinned_words_acquire();
     for (auto& e : ev_occ_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
   } catch (...) {
     release();
@@ -451,17 +494,8 @@ void GpuSolver::release() {
   if (stream_) cudaStreamSynchronize(stream_);
   cudaFree(d_tables_);
   cudaFree(d_slots_);
-  cudaFree(d_state_);
-  cudaFree(d_cand_score_);
-  cudaFree(d_cand_slot_);
-  cudaFree(d_hsub_);
-  cudaFree(d_err_);
-  cudaFree(d_occ_);
-  cudaFree(d_sect_);
-  cudaFree(d_part_key_);
-  cudaFree(d_part_slot_);
-  cudaFree(d_part_sum_);
-  cudaFree(d_done_);
+  cudaFree(d_misc_);
+  d_misc_ = nullptr;
   d_sect_ = nullptr;
   d_part_key_ = nullptr;
   d_part_slot_ = nullptr;
@@ -475,7 +509,7 @@ void GpuSolver::release() {
   d_hsub_ = nullptr;
   d_err_ = nullptr;
   d_occ_ = nullptr;
-  if (h_occ_) cudaFreeHost(h_occ_);
+  if (h_occ_) pinned_words_release(h_occ_);
   h_occ_ = nullptr;
   for (auto& e : ev_occ_) {
     if (e) cudaEventDestroy(e);

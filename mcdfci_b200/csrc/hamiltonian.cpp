@@ -39,12 +39,13 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
   auto spin = [](int so) { return so & 1; };
   auto sp = [](int so) { return so >> 1; };
 
-  // Reject couplings between alpha and beta spin-orbitals.
-  for (int i = 0; i < nso; ++i)
+  // Reject couplings between alpha and beta spin-orbitals (an RHF file's
+  // expansion has none; UHF files and arrays from the C ABI are checked).
+  for (int i = 0; i < nso && !fci.spin_conserving; ++i)
     for (int a = 0; a < nso; ++a)
       if (spin(i) != spin(a) && std::fabs(fci.h(i, a)) > thr)
         throw std::invalid_argument("one-electron integrals couple alpha and beta spin-orbitals.");
-  for (int i = 0; i < nso; ++i)
+  for (int i = 0; i < nso && !fci.spin_conserving; ++i)
     for (int j = i; j < nso; ++j)
       for (int a = 0; a < nso; ++a)
         for (int b = 0; b < nso; ++b) {

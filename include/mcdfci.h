@@ -96,13 +96,16 @@ typedef struct mcd_options {
    * reserves its table.  A growth that finds the device memory taken by
    * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
   int32_t table_growth;
-  /* 2 (default): each subspace eigenproblem is first solved by shifted
+  /* 0 (default): every subspace eigenproblem by the full reduction
+   * (Householder, multisection, inverse iteration).  2: first by shifted
    * inverse iteration (a Cholesky factorisation of B - sigma I, sigma below
    * the current energy by 16 times the last energy drop, certifies sigma <
    * lambda_1; the current vector starts it), its steps run by one warp on the
    * explicit inverse, with the full reduction when that fails; 1: the same
-   * with block-wide steps; 0: the full reduction every time.  No counterpart
-   * in the reference (LAPACK dsyevr, src/solver.h:400-411). */
+   * with block-wide steps.  On 24 orbitals, k = 32, the shifted solver costs
+   * as much as the reduction late in a solve and more early on (it needs
+   * more steps while the energy still drops fast), hence the default.  No
+   * counterpart in the reference (LAPACK dsyevr, src/solver.h:400-411). */
   int32_t eig_shift;
 } mcd_options;
 

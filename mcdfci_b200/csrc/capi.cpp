@@ -195,7 +195,7 @@ void mcd_options_default(mcd_options* o) {
   o->groups = 0;
   o->compaction = 0;
   o->table_growth = 1;
-  o->eig_shift = 2;
+  o->eig_shift = 0;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;

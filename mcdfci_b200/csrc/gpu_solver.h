@@ -34,10 +34,10 @@ struct SolverOptions {
   // allocation) as it fills, up to the size max_memory gives; false: the
   // whole table is allocated at creation, as the reference reserves it.
   bool table_growth = true;
-  // Subspace eigenproblem: 2 shifted inverse iteration first, its steps by
-  // one warp on the explicit inverse; 1 the same with block-wide steps; 0 the
-  // full reduction every time.
-  int eig_shift = 2;
+  // Subspace eigenproblem: 0 the full reduction every time; 2 shifted
+  // inverse iteration first, its steps by one warp on the explicit inverse;
+  // 1 the same with block-wide steps.
+  int eig_shift = 0;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;

@@ -212,6 +212,8 @@ int mcd_batch_reset(mcd_batch* b);
 int mcd_batch_run_iterations(mcd_batch* b, int64_t n);
 int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, double* column_ms, double* total_ms);
 int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r);
+/* mcd_residual of one instance: ||H c - E c|| / ||c|| of its current vector. */
+int mcd_batch_residual(mcd_batch* b, int32_t instance, double* residual);
 /* Energies of the last batch solve, one per instance. */
 int mcd_batch_result(const mcd_batch* b, double* energies);
 

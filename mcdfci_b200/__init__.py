@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
-    "mcd_debug_table_info", "mcd_debug_setup_times",
+    "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual",
 )
 
 
@@ -168,6 +168,7 @@ def library() -> ctypes.CDLL:
     L.mcd_residual.argtypes = [vp, _dp]
     L.mcd_debug_table_info.argtypes = [vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_setup_times.argtypes = [vp, _dp, ctypes.c_int32]
+    L.mcd_batch_residual.argtypes = [vp, ctypes.c_int32, _dp]
     L.mcd_debug_slots.argtypes = [vp, _u64p, _u64p, _dp, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
@@ -627,6 +628,12 @@ class CDFCIBatch:
         r = mcd_report()
         _check(library().mcd_batch_get_report(self._h, int(i), ctypes.byref(r)))
         return r.as_dict()
+
+    def residual(self, i: int) -> float:
+        """||H c - E c|| / ||c|| of instance i's current vector."""
+        r = ctypes.c_double()
+        _check(library().mcd_batch_residual(self._h, int(i), ctypes.byref(r)))
+        return r.value
 
 
 def _eig_inputs(hsub, x, z):

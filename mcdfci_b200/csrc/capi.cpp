@@ -319,6 +319,15 @@ int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, d
   });
 }
 
+int mcd_batch_residual(mcd_batch* b, int32_t instance, double* residual) {
+  return guarded([&] {
+    if (!b || !residual) return fail(MCD_ERR_INVALID, "NULL argument.");
+    if (instance < 0 || instance >= b->impl->size()) return fail(MCD_ERR_INVALID, "instance out of range.");
+    *residual = b->impl->instance(instance).residual();
+    return MCD_OK;
+  });
+}
+
 int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r) {
   return guarded([&] {
     if (!b || !r) return fail(MCD_ERR_INVALID, "NULL argument.");

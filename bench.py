@@ -568,8 +568,11 @@ def b200_arm(args, rank, world, local_rank):
     try:
         path = write_workload(tmp, args.seed)
         fc = mc.Fcidump(path)
+        # num_iterations: the iterations this run makes (the first table is
+        # sized for them, up to two 64-iteration chunks).
         solver = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
-                          z_threshold=args.z_threshold, threshold=0.0, device=local_rank, groups=args.groups)
+                          z_threshold=args.z_threshold, threshold=0.0, device=local_rank, groups=args.groups,
+                          num_iterations=args.warmup + 2 * args.steps + max(args.aged_iterations, 0) + args.aged_steps)
         solver.reset()
         solver.run_iterations(args.warmup)
         r0 = solver.report()
@@ -731,6 +734,7 @@ def e2e_run(mc, fc, args, local_rank):
         "create_host_tables_ms": stages["host_tables"],
         "create_device_alloc_ms": stages["device_alloc"],
         "create_upload_ms": stages["upload"],
+        "create_device_setup_ms": stages["device_setup"],
         "solve_ms": 1000.0 * dt - create_ms,
         "solve_table_fill_ms": stages["table_fill"],
         "solve_graph_build_ms": stages["graph_build"],

@@ -89,8 +89,8 @@ typedef struct mcd_options {
    * it is below 40%, instead of failing with MCD_ERR_OVERFLOW.  0 by default. */
   int32_t compaction;
   /* 1 (default): the hash table starts at the size two 64-iteration chunks
-   * of worst-case inserts need (k whole columns per iteration, kept below 3/4
-   * full) and doubles, rehashing into a new allocation between chunks, up to
+   * (or num_iterations, when fewer) of worst-case inserts need (k whole
+   * columns per iteration, kept below 3/4 full) and doubles, rehashing into a new allocation between chunks, up to
    * the table max_memory gives; occupancy limits and results are those of the
    * full table.  0: the full table is allocated at creation, as the reference
    * reserves its table.  A growth that finds the device memory taken by
@@ -310,7 +310,8 @@ int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_
  * them: 0 Hamiltonian tables and reference determinant (host), 1 device
  * allocations at creation, 2 table upload, 3 table fill of the last reset
  * (synchronised), 4 CUDA graph builds, 5 table growths, 6 report read-backs,
- * summed since creation.  No counterpart in the reference. */
+ * 7 device and stream set-up, summed since creation.  No counterpart in the
+ * reference. */
 int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n);
 /* Launch shape of the column kernel: CTAs per column, length of the per-CTA
  * candidate lists, and entries per Hamiltonian column.  No counterpart in the

@@ -474,7 +474,8 @@ class CDFCI:
                                         h.ctypes.data_as(_dp)))
         return h.reshape(k, k)
 
-    SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports")
+    SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports",
+                    "device_setup")
 
     def table_info(self) -> dict:
         c, mc, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()

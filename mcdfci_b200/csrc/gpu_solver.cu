@@ -334,6 +334,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     throw McdError(MCD_ERR_UNSUPPORTED, "max_memory asks for more than 2^32 hash slots (128 GB).");
 
   // Device.
+  const auto t_dev = clock::now();
   if (opt_.device >= 0) check(cudaSetDevice(opt_.device), "cudaSetDevice");
   check(cudaGetDevice(&device_), "cudaGetDevice");
   if (opt_.stream) {
@@ -356,13 +357,16 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
     const size_t margin = static_cast<size_t>(1) << 30;
     budget_slots_ = free_b > margin ? (free_b - margin) / sizeof(Slot) : 0;
-    const double per_chunk =
-        (2.0 * static_cast<double>(graph_iters_) * opt_.k + 1.0) * static_cast<double>(entries_);
+    // (or num_iterations, when a solve asks for fewer)
+    const double first_iters = static_cast<double>(
+        std::min<long long>(2 * graph_iters_, std::max<long long>(1, opt_.num_iterations)));
+    const double per_chunk = (first_iters * opt_.k + 1.0) * static_cast<double>(entries_);
     size_t c = static_cast<size_t>(1) << 16;
     while (c < max_capacity_ && 0.75 * static_cast<double>(c) < per_chunk) c <<= 1;
     if (!opt_.table_growth || c >= max_capacity_ || c + max_capacity_ > budget_slots_) c = max_capacity_;
     capacity_ = c;
   }
+  setup_ms_[7] = ms_since(t_dev);
 
   auto t_alloc = clock::now();
   double upload_ms = 0.0;

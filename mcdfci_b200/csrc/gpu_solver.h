@@ -119,8 +119,9 @@ class GpuSolver {
   // 0 Hamiltonian tables and reference determinant on the host, 1 device
   // allocations of the constructor, 2 table upload, 3 table fill of the last
   // reset (synchronised), 4 CUDA graph builds, 5 table growths, 6 report
-  // read-backs (finish, state copy, synchronisation), summed since creation.
-  static constexpr int kSetupStages = 7;
+  // read-backs (finish, state copy, synchronisation), 7 device and stream
+  // set-up (device, stream, attributes, free memory), summed since creation.
+  static constexpr int kSetupStages = 8;
   const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }

@@ -31,9 +31,9 @@ pytestmark = pytest.mark.gpu
 RESIDUAL = 1e-9
 STEP = 1e-5
 ENTRIES = 64
-K = 16
-CHUNK = 4000
-MAX_ITERATIONS = 200000
+K = 32
+CHUNK = 8000
+MAX_ITERATIONS = 400000
 OPTS = dict(num_of_coordinate=K, estimate=K, max_memory=0.1, threshold=0.0, z_threshold=0.0)
 
 

@@ -403,12 +403,13 @@ def phases_arm(args, local_rank):
                    "merge": round(col.pop("merge") / merges)}
         scatter = []
         if args.scatter_sweep:
-            for entries in (527072, 2108288, 8433152, 33732608):
-                for cps in (3, 8):
-                    for ilp in (1, 4):
-                        r = s.scatter_rate(entries, 10, ilp, cps)
-                        scatter.append({"slots": entries, "ctas_per_sm": cps, "ilp": ilp, "slots_per_s": r,
-                                        "us_per_launch": entries / r * 1e6})
+            for mode, name in enumerate(s.SCATTER_MODES):
+                for entries in (527072, 8433152):
+                    for cps in (3, 8):
+                        for ilp in (1, 4):
+                            r = s.scatter_rate(entries, 10, ilp, cps, mode)
+                            scatter.append({"mode": name, "slots": entries, "ctas_per_sm": cps, "ilp": ilp,
+                                            "slots_per_s": r, "us_per_launch": entries / r * 1e6})
         rep = s.report()
         eig = {"shifted_updates": rep["inv_updates"] - rb["inv_updates"],
                "shifted_steps_avg": (rep["inv_steps"] - rb["inv_steps"]) / max(1, rep["inv_updates"] - rb["inv_updates"]),

@@ -325,6 +325,13 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
  * No counterpart in the reference. */
 int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
                            double* slots_per_s);
+/* mcd_debug_scatter_rate with the slot touched in one of four ways, to split
+ * the ceiling between its parts: mode 0 as a column entry (key, x, atomic
+ * add with return), 1 key and x loads only, 2 the atomic with return only,
+ * 3 the key load and an atomic add whose return is unused.  No counterpart
+ * in the reference. */
+int mcd_debug_scatter_rate_mode(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
+                                int32_t mode, double* slots_per_s);
 /* SM cycles spent in each phase of the leader kernel (21 phases: state load,
  * finish, candidate gather, top-k, tie sort, picked, H_sub, update_x, publish,
  * eig setup, tridiagonalisation, multisection, inverse iteration,

@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
-    "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual",
+    "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual", "mcd_debug_scatter_rate_mode",
 )
 
 
@@ -169,6 +169,8 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_table_info.argtypes = [vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_setup_times.argtypes = [vp, _dp, ctypes.c_int32]
     L.mcd_batch_residual.argtypes = [vp, ctypes.c_int32, _dp]
+    L.mcd_debug_scatter_rate_mode.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, _dp]
     L.mcd_debug_slots.argtypes = [vp, _u64p, _u64p, _dp, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
@@ -529,13 +531,16 @@ class CDFCI:
         _check(library().mcd_debug_leader_sections(self._h, v.ctypes.data_as(_u64p), len(v)))
         return {name: int(c) for name, c in zip(self.LEADER_SECTIONS, v)}
 
-    def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1, ctas_per_sm: int = 0) -> float:
-        """Slots per second of the table's scattered-access probe (a column
-        entry's key read, x read and atomic z add, at pseudo-random slots),
-        with ctas_per_sm CTAs of 256 threads per SM (0: 8)."""
+    SCATTER_MODES = ("key_x_atomic", "key_x_loads", "atomic_only", "key_and_reduction")
+
+    def scatter_rate(self, entries: int, reps: int = 20, ilp: int = 1, ctas_per_sm: int = 0, mode: int = 0) -> float:
+        """Slots per second of the table's scattered-access probe (mode 0: a
+        column entry's key read, x read and atomic z add, at pseudo-random
+        slots; see SCATTER_MODES), with ctas_per_sm CTAs of 256 threads per
+        SM (0: 8)."""
         r = ctypes.c_double()
-        _check(library().mcd_debug_scatter_rate(self._h, int(entries), int(reps), int(ilp), int(ctas_per_sm),
-                                                ctypes.byref(r)))
+        _check(library().mcd_debug_scatter_rate_mode(self._h, int(entries), int(reps), int(ilp), int(ctas_per_sm),
+                                                     int(mode), ctypes.byref(r)))
         return r.value
 
     def launch_info(self) -> dict:

@@ -691,6 +691,16 @@ int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_
   });
 }
 
+int mcd_debug_scatter_rate_mode(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
+                                int32_t mode, double* slots_per_s) {
+  return guarded([&] {
+    if (!s || !slots_per_s) return fail(MCD_ERR_INVALID, "NULL argument.");
+    if (mode < 0 || mode > 3) return fail(MCD_ERR_INVALID, "mode must be 0..3.");
+    *slots_per_s = s->impl->scatter_rate(entries, reps, ilp, ctas_per_sm, mode);
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t ilp, int32_t ctas_per_sm,
                            double* slots_per_s) {
   return guarded([&] {

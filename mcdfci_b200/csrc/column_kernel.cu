@@ -775,7 +775,11 @@ cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s) {
 // its slot (the 16-byte key, then x and an FP64 atomic add on z that returns
 // the old value; the add is of zero, so the table keeps its values).  ILP
 // slots are in flight per thread; the grid fills every SM.
-template <int ILP>
+// MODE 0: the 16-byte key, x and an FP64 atomic add of zero with its return,
+// as a column entry touches its slot; 1: key and x loads only; 2: the atomic
+// with return only; 3: key load and an atomic add whose return is unused
+// (a reduction, no round trip).
+template <int ILP, int MODE>
 __global__ void __launch_bounds__(256) scatter_probe_kernel(Slot* slots, uint64_t mask, long long entries,
                                                             uint64_t seed, double* sink) {
   double acc = 0.0;
@@ -786,26 +790,42 @@ __global__ void __launch_bounds__(256) scatter_probe_kernel(Slot* slots, uint64_
 #pragma unroll
     for (int q = 0; q < ILP; ++q) {
       sl[q] = fmix64(seed ^ static_cast<uint64_t>(e0 + q)) & mask;
-      if (e0 + q < entries) load_key(slots + sl[q], ka[q], kb[q]);
+      ka[q] = kb[q] = 0;
+      if (MODE != 2 && e0 + q < entries) load_key(slots + sl[q], ka[q], kb[q]);
     }
 #pragma unroll
     for (int q = 0; q < ILP; ++q) {
       if (e0 + q < entries && ka[q] != ~0ull - 1ull) {  // uses the key, as a probe does
         Slot* sp = slots + sl[q];
-        acc += sp->x + atomicAdd(&sp->z, 0.0) + static_cast<double>(kb[q] & 1ull);
+        if (MODE == 0) acc += sp->x + atomicAdd(&sp->z, 0.0) + static_cast<double>(kb[q] & 1ull);
+        if (MODE == 1) acc += sp->x + static_cast<double>(kb[q] & 1ull);
+        if (MODE == 2) acc += atomicAdd(&sp->z, 0.0);
+        if (MODE == 3) {
+          atomicAdd(&sp->z, 0.0);
+          acc += static_cast<double>(kb[q] & 1ull);
+        }
       }
     }
   }
   if (acc == 1234.5678) *sink = acc;  // keeps the loads
 }
 
-cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
-                          cudaStream_t s) {
-  if (ctas < 1) return cudaErrorInvalidValue;
+template <int MODE>
+void scatter_probe_mode(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
+                        cudaStream_t s) {
   if (ilp >= 4)
-    scatter_probe_kernel<4><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
+    scatter_probe_kernel<4, MODE><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
   else
-    scatter_probe_kernel<1><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
+    scatter_probe_kernel<1, MODE><<<ctas, 256, 0, s>>>(t.slots, t.mask, entries, seed, sink);
+}
+
+cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
+                          cudaStream_t s, int mode) {
+  if (ctas < 1 || mode < 0 || mode > 3) return cudaErrorInvalidValue;
+  if (mode == 0) scatter_probe_mode<0>(t, entries, ilp, ctas, seed, sink, s);
+  if (mode == 1) scatter_probe_mode<1>(t, entries, ilp, ctas, seed, sink, s);
+  if (mode == 2) scatter_probe_mode<2>(t, entries, ilp, ctas, seed, sink, s);
+  if (mode == 3) scatter_probe_mode<3>(t, entries, ilp, ctas, seed, sink, s);
   return cudaGetLastError();
 }
 

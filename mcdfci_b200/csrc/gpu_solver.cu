@@ -1365,7 +1365,7 @@ std::vector<unsigned long long> GpuSolver::column_sections(bool enable) {
   return v;
 }
 
-double GpuSolver::scatter_rate(long long entries, int reps, int ilp, int ctas_per_sm) {
+double GpuSolver::scatter_rate(long long entries, int reps, int ilp, int ctas_per_sm, int mode) {
   if (entries <= 0 || reps <= 0) throw McdError(MCD_ERR_INVALID, "entries and reps must be positive.");
   if (ctas_per_sm < 0 || ctas_per_sm > 8) throw McdError(MCD_ERR_INVALID, "ctas_per_sm must be in 0..8.");
   int sms = 0;
@@ -1377,10 +1377,11 @@ double GpuSolver::scatter_rate(long long entries, int reps, int ilp, int ctas_pe
   try {
     check(cudaEventCreate(&e0), "cudaEventCreate");
     check(cudaEventCreate(&e1), "cudaEventCreate");
-    check(scatter_probe(td_, entries, ilp, ctas, 0x5eedull, sink, stream_), "scatter probe");
+    check(scatter_probe(td_, entries, ilp, ctas, 0x5eedull, sink, stream_, mode), "scatter probe");
     check(cudaEventRecord(e0, stream_), "cudaEventRecord");
     for (int r = 0; r < reps; ++r)
-      check(scatter_probe(td_, entries, ilp, ctas, 0x5eedull + 7919ull * (r + 1), sink, stream_), "scatter probe");
+      check(scatter_probe(td_, entries, ilp, ctas, 0x5eedull + 7919ull * (r + 1), sink, stream_, mode),
+            "scatter probe");
     check(cudaEventRecord(e1, stream_), "cudaEventRecord");
     check(cudaEventSynchronize(e1), "cudaEventSynchronize");
     check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");

@@ -108,7 +108,7 @@ class GpuSolver {
   // Slots per second of the scattered-access probe on this solver's table
   // (reps timed launches of `entries` slots after one untimed launch), with
   // ctas_per_sm CTAs of 256 threads per SM (0: 8, every thread slot).
-  double scatter_rate(long long entries, int reps, int ilp, int ctas_per_sm);
+  double scatter_rate(long long entries, int reps, int ilp, int ctas_per_sm, int mode = 0);
 
   const HamHost& ham() const { return ham_; }
   Det reference_det() const { return ref_; }

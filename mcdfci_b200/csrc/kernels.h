@@ -200,8 +200,10 @@ cudaError_t launch_rdm(const RdmLaunch& r, cudaStream_t s);
 // read (key, x) and given an atomic add of zero on z; ilp 1 or 4 slots in
 // flight per thread; `ctas` CTAs of 256 threads.  `sink`: one device double,
 // written only to keep loads.
+// mode 0: key, x and atomic with return; 1: key and x only; 2: atomic with
+// return only; 3: key and an atomic add without return.
 cudaError_t scatter_probe(const TableDev& t, long long entries, int ilp, int ctas, uint64_t seed, double* sink,
-                          cudaStream_t s);
+                          cudaStream_t s, int mode = 0);
 cudaError_t debug_column(const HamDev& h, Det d, double hdiag, uint64_t* a_out, uint64_t* b_out,
                          double* v_out, int cap, int* n_out, cudaStream_t s);
 cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cudaStream_t s);

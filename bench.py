@@ -88,6 +88,7 @@ def parse_args():
     ap.add_argument("--aged-iterations", type=int, default=2000,
                     help="iterations in all before the aged-table timing (0: skip it)")
     ap.add_argument("--aged-steps", type=int, default=256)
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner object")
     ap.add_argument("--phases", action="store_true",
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
@@ -473,6 +474,29 @@ def curve_sharded_arm(args, rank, world, local_rank):
     return 0
 
 
+def autotune_object(mc, tmp, args, local_rank):
+    """CTAs per column chosen by the autotuner against the fixed rule, from
+    its timed trials (16 iterations per candidate, column-kernel device time),
+    on three workloads."""
+    from mcdfci_b200 import synth
+
+    out = {}
+    for name, k, mem, zt in (("n24_6a6b", 32, 8.0, 1e-9), ("n16_5a5b", 16, 1.0, 0.0), ("n42_24a24b", 64, 32.0, 1e-6)):
+        p = os.path.join(tmp, f"tune_{name}.fcidump")
+        synth.write_fcidump(p, name, seed=args.seed)
+        s = mc.CDFCI(mc.Fcidump(p), num_of_coordinate=k, estimate=k, max_memory=mem, z_threshold=zt, threshold=0.0,
+                     device=local_rank, autotune=True, num_iterations=256)
+        s.reset()
+        s.run_iterations(16 * 10)
+        info = s.autotune_info()
+        s.close()
+        rule_us = next((t["column_us"] for t in info["trials"] if t["groups"] == info["rule"]), None)
+        best_us = min((t["column_us"] for t in info["trials"]), default=None)
+        out[name] = {"k": k, "rule_groups": info["rule"], "chosen_groups": info["chosen"],
+                     "rule_column_us": rule_us, "chosen_column_us": best_us, "trials": info["trials"]}
+    return out
+
+
 def write_workload(d, seed):
     from mcdfci_b200 import synth
 
@@ -664,6 +688,10 @@ def b200_arm(args, rank, world, local_rank):
             if dist:
                 e2e["value"] = replica_rate(args.k * e2e["iterations"], e2e["seconds"], world, dist, "cuda")
 
+        tuned = None
+        if not args.no_autotune:
+            tuned = autotune_object(mc, tmp, args, local_rank)
+
         batched = None
         if not args.no_batched:
             ctmp = tempfile.mkdtemp(prefix="mcd_curve_", dir=tmp)
@@ -704,6 +732,7 @@ def b200_arm(args, rank, world, local_rank):
                 "energy": r1["energy"],
                 "z_size": r1["z_size"],
                 "aged": aged,
+                "autotune": tuned,
                 "e2e_detail": e2e,
             }
             print(json.dumps(out))

@@ -107,6 +107,13 @@ typedef struct mcd_options {
    * more steps while the energy still drops fast), hence the default.  No
    * counterpart in the reference (LAPACK dsyevr, src/solver.h:400-411). */
   int32_t eig_shift;
+  /* 1: with groups = 0, the CTAs per Hamiltonian column are chosen from
+   * timed trials the first time at least 16 iterations per candidate are run
+   * (the trials are iterations of the solve), among values around the fixed
+   * rule's, the fastest column kernel kept and remembered for the process
+   * per (orbitals, electrons, k, m, SM count).  0 (default): the fixed rule.
+   * No counterpart in the reference. */
+  int32_t autotune;
 } mcd_options;
 
 /* One line of the reference's report table (src/solver.h:761-798). */
@@ -313,6 +320,12 @@ int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_
  * 7 device and stream set-up, summed since creation.  No counterpart in the
  * reference. */
 int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n);
+/* The autotuner's record: the fixed rule's CTAs per column, the chosen
+ * ones, and up to cap trials (CTAs per column, column-kernel microseconds
+ * per iteration); *n receives the number of trials (0 before tuning, or
+ * when the choice came from the process's cache). */
+int mcd_debug_autotune_info(const mcd_solver* s, int32_t* rule, int32_t* chosen, int32_t* trial_groups,
+                            double* trial_us, int32_t cap, int32_t* n);
 /* Launch shape of the column kernel: CTAs per column, length of the per-CTA
  * candidate lists, and entries per Hamiltonian column.  No counterpart in the
  * reference (it has no GPU launch). */

@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
     "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual", "mcd_debug_scatter_rate_mode",
+    "mcd_debug_autotune_info",
 )
 
 
@@ -77,7 +78,7 @@ class mcd_options(ctypes.Structure):
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
-        ("table_growth", ctypes.c_int32), ("eig_shift", ctypes.c_int32),
+        ("table_growth", ctypes.c_int32), ("eig_shift", ctypes.c_int32), ("autotune", ctypes.c_int32),
     ]
 
 
@@ -169,6 +170,9 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_table_info.argtypes = [vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_setup_times.argtypes = [vp, _dp, ctypes.c_int32]
     L.mcd_batch_residual.argtypes = [vp, ctypes.c_int32, _dp]
+    L.mcd_debug_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_int32), _dp, ctypes.c_int32,
+                                          ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_scatter_rate_mode.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                               ctypes.c_int32, _dp]
     L.mcd_debug_slots.argtypes = [vp, _u64p, _u64p, _dp, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
@@ -304,7 +308,7 @@ def make_options(**kw) -> mcd_options:
             o.z_threshold_search = int(bool(v))
         elif k == "eig_shift":
             o.eig_shift = int(v)
-        elif k in ("compaction", "table_growth"):
+        elif k in ("compaction", "table_growth", "autotune"):
             setattr(o, k, int(bool(v)))
         else:
             setattr(o, k, v)
@@ -478,6 +482,15 @@ class CDFCI:
 
     SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports",
                     "device_setup")
+
+    def autotune_info(self) -> dict:
+        rule, chosen, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        g = (ctypes.c_int32 * 16)()
+        us = (ctypes.c_double * 16)()
+        _check(library().mcd_debug_autotune_info(self._h, ctypes.byref(rule), ctypes.byref(chosen), g, us, 16,
+                                                 ctypes.byref(n)))
+        return {"rule": rule.value, "chosen": chosen.value,
+                "trials": [{"groups": g[i], "column_us": us[i]} for i in range(min(n.value, 16))]}
 
     def table_info(self) -> dict:
         c, mc, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()

@@ -74,6 +74,7 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.table_growth = o->table_growth != 0;
   if (o->eig_shift < 0 || o->eig_shift > 2) throw mcd::McdError(MCD_ERR_INVALID, "eig_shift must be 0, 1 or 2.");
   s.eig_shift = o->eig_shift;
+  s.autotune = o->autotune != 0;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -159,6 +160,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   if (cd.has("compaction")) o->compaction = cd.at("compaction").as_bool("compaction") ? 1 : 0;
   if (cd.has("table_growth")) o->table_growth = cd.at("table_growth").as_bool("table_growth") ? 1 : 0;
   if (cd.has("eig_shift")) o->eig_shift = static_cast<int32_t>(cd.at("eig_shift").as_number("eig_shift"));
+  if (cd.has("autotune")) o->autotune = cd.at("autotune").as_bool("autotune") ? 1 : 0;
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -196,6 +198,7 @@ void mcd_options_default(mcd_options* o) {
   o->compaction = 0;
   o->table_growth = 1;
   o->eig_shift = 0;
+  o->autotune = 0;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;
@@ -706,6 +709,22 @@ int mcd_debug_scatter_rate(mcd_solver* s, int64_t entries, int32_t reps, int32_t
   return guarded([&] {
     if (!s || !slots_per_s) return fail(MCD_ERR_INVALID, "NULL argument.");
     *slots_per_s = s->impl->scatter_rate(entries, reps, ilp, ctas_per_sm);
+    return MCD_OK;
+  });
+}
+
+int mcd_debug_autotune_info(const mcd_solver* s, int32_t* rule, int32_t* chosen, int32_t* trial_groups,
+                            double* trial_us, int32_t cap, int32_t* n) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    if (rule) *rule = s->impl->groups_rule();
+    if (chosen) *chosen = s->impl->groups();
+    const auto& t = s->impl->tune_trials();
+    if (n) *n = static_cast<int32_t>(t.size());
+    for (int32_t i = 0; i < cap && i < static_cast<int32_t>(t.size()); ++i) {
+      if (trial_groups) trial_groups[i] = t[i].first;
+      if (trial_us) trial_us[i] = t[i].second;
+    }
     return MCD_OK;
   });
 }

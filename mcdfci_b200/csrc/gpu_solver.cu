@@ -10,6 +10,7 @@
 #include <cstring>
 #include <iomanip>
 #include <iostream>
+#include <map>
 #include <mutex>
 #include <sstream>
 
@@ -345,7 +346,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   }
   int sms = 0;
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "cudaDeviceGetAttribute");
-  groups_ = opt_.groups > 0 ? opt_.groups : column_groups(entries_, opt_.k, opt_.fill_gpu ? 3 * sms : 0);
+  groups_rule_ = column_groups(entries_, opt_.k, opt_.fill_gpu ? 3 * sms : 0);
+  groups_ = opt_.groups > 0 ? opt_.groups : groups_rule_;
+  if (opt_.autotune && opt_.groups == 0 && groups_ > kMaxGroups) groups_ = kMaxGroups;
   list_ = column_list_size(opt_.m);
 
   // First table: large enough that two graphs' worth of iterations, each
@@ -415,7 +418,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
 
     d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
     // The iteration's small buffers in one allocation.
-    const size_t parts = static_cast<size_t>(opt_.k) * groups_;
+    // Per-CTA partial lists for the largest CTA count the autotuner tries.
+    const size_t parts = static_cast<size_t>(opt_.k) * std::max(groups_, opt_.autotune ? kMaxGroups : 1);
     const size_t mk = static_cast<size_t>(kMaxK) * opt_.m;
     size_t mo = 0;
     auto carve = [&](size_t bytes) {
@@ -675,7 +679,65 @@ void GpuSolver::launch_chunk(long long n) {
   }
 }
 
+namespace {
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_tune_cache;  // (norb, na, nb, k, m, SMs) -> CTAs per column
+}  // namespace
+
+void GpuSolver::set_groups(int g) {
+  if (g == groups_) return;
+  groups_ = g;
+  cl_.groups = g;
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+}
+
+long long GpuSolver::autotune_groups(long long budget) {
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "cudaDeviceGetAttribute");
+  const std::vector<int> key{ham_.norb, na_, nb_, opt_.k, opt_.m, sms};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      set_groups(it->second);
+      tuned_ = true;
+      return 0;
+    }
+  }
+  // Candidates around the rule, within 1..kMaxGroups.
+  std::vector<int> cand;
+  for (int g : {groups_rule_, groups_rule_ / 2, groups_rule_ * 2, groups_rule_ * 3 / 4, groups_rule_ * 3 / 2, 8, 16,
+                32, 64}) {
+    g = std::max(1, std::min(g, kMaxGroups));
+    if (std::find(cand.begin(), cand.end(), g) == cand.end()) cand.push_back(g);
+  }
+  if (budget < kTuneIters * static_cast<long long>(cand.size())) return 0;  // not enough iterations yet
+  tuned_ = true;
+  long long done = 0;
+  int best = groups_;
+  double best_us = 1e300;
+  tune_trials_.clear();
+  for (int g : cand) {
+    set_groups(g);
+    double lead = 0.0, col = 0.0, tot = 0.0;
+    run_iterations_timed(kTuneIters, &lead, &col, &tot);
+    done += kTuneIters;
+    const double us = 1000.0 * col / kTuneIters;
+    tune_trials_.push_back({g, us});
+    if (us < best_us) {
+      best_us = us;
+      best = g;
+    }
+  }
+  set_groups(best);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_cache[key] = best;
+  return done;
+}
+
 void GpuSolver::run_iterations(long long n) {
+  if (opt_.autotune && !tuned_ && opt_.groups == 0) n -= autotune_groups(n);
   while (n > 0) {
     const long long c = std::min(n, graph_iters_);
     ensure_room(c);

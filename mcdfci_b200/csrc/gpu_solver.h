@@ -38,6 +38,10 @@ struct SolverOptions {
   // inverse iteration first, its steps by one warp on the explicit inverse;
   // 1 the same with block-wide steps.
   int eig_shift = 0;
+  // Choose the CTAs per Hamiltonian column from timed trials (real
+  // iterations of the solve) the first time enough iterations are run, and
+  // remember the choice per (orbitals, electrons, k, m, SM count).
+  bool autotune = false;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -125,6 +129,8 @@ class GpuSolver {
   const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }
+  int groups_rule() const { return groups_rule_; }
+  const std::vector<std::pair<int, double>>& tune_trials() const { return tune_trials_; }
   // Launch descriptors and the column CTA count, for running this instance
   // inside a batch (GpuBatch) on the same stream.
   const LeaderLaunch& leader_launch() const { return ll_; }
@@ -150,6 +156,10 @@ class GpuSolver {
   size_t next_capacity(size_t c) const;     // the capacity after c
   void record_occupancy(long long iters);   // async occupancy read after a chunk of iters
   void launch_chunk(long long n);           // n <= graph_iters_ iterations, graph or direct
+  // The autotuner: trials of kTuneIters iterations per candidate CTA count,
+  // the fastest column kernel kept; returns the iterations it ran.
+  long long autotune_groups(long long budget);
+  void set_groups(int g);
 
   SolverOptions opt_;
   HamHost ham_;
@@ -161,6 +171,9 @@ class GpuSolver {
   size_t max_capacity_ = 0;         // hash slots max_memory gives (the reference's table)
   size_t budget_slots_ = 0;         // device memory for two tables at once, in slots
   int growths_ = 0;
+  int groups_rule_ = 1;      // the CTAs per column the fixed rule gives
+  bool tuned_ = false;
+  std::vector<std::pair<int, double>> tune_trials_;  // (CTAs per column, column kernel us per iteration)
   double setup_ms_[kSetupStages] = {};
   // Occupancy reads after the last two chunks: pinned host words, events, and
   // the iterations enqueued since the reset when each was recorded.

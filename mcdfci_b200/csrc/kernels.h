@@ -170,6 +170,9 @@ int column_list_size(int m);
 // such columns would leave some of `resident` CTA slots of the GPU empty
 // (resident = 0: never more); at most 96.
 int column_groups(int entries, int k, int resident);
+// The most CTAs per column the autotuner tries, and its iterations per trial.
+constexpr int kMaxGroups = 96;
+constexpr int kTuneIters = 16;
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
 // Sets, on the current device, the launch attribute launch_leader needs for

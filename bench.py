@@ -387,7 +387,7 @@ def phases_arm(args, local_rank):
         synth.write_fcidump(path, args.phase_workload, seed=args.seed)
         s = mc.CDFCI(mc.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                      z_threshold=args.z_threshold, threshold=0.0, groups=args.groups, device=local_rank,
-                     eig_shift=args.eig_shift)
+                     eig_shift=args.eig_shift, num_iterations=args.warmup + args.steps)
         s.reset()
         s.run_iterations(args.warmup)
         rb = s.report()

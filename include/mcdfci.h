@@ -203,7 +203,8 @@ int mcd_scalars(mcd_solver* s, double xx[2], double scale[2], double xz[2], int6
  * of a binding curve) one after another with separate runs
  * (experiments/4.4-binding-curve/dissociation.sh:2-9).  A batch holds up to 64
  * instances, each an FCIDUMP of its own size with its own hash wavefunction
- * of options->max_memory GB, all with the same options (k, m, z_threshold,
+ * of options->max_memory GB (the tables carved from one device allocation,
+ * committed at creation), all with the same options (k, m, z_threshold,
  * num_iterations, report_interval; z_threshold_search is not supported).  One
  * iteration advances every instance with two launches: one leader CTA per
  * instance and the column CTAs of all instances in one grid; each instance

@@ -48,6 +48,18 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       groups_[g].lb->n = groups_[g].cb->n = 0;
       groups_[g].cb->cta_begin[0] = 0;
     }
+    // The instances' tables carved from one allocation, each a power of two
+    // of 32-byte slots (so every table starts aligned).
+    std::vector<size_t> caps(fcis.size());
+    size_t total = 0;
+    for (size_t i = 0; i < fcis.size(); ++i) total += caps[i] = GpuSolver::full_capacity(*fcis[i], opt_.max_memory);
+    void* pool = nullptr;
+    cudaError_t ae = cudaMalloc(&pool, total * sizeof(Slot));
+    if (ae != cudaSuccess)
+      throw McdError(MCD_ERR_CUDA, "cudaMalloc(batch tables, " + std::to_string(total * sizeof(Slot)) +
+                                       " bytes): " + cudaGetErrorString(ae));
+    pool_ = static_cast<Slot*>(pool);
+    size_t off = 0;
     // Instance i goes to group i % ng, on that group's stream.
     for (size_t i = 0; i < fcis.size(); ++i) {
       Group& G = groups_[i % static_cast<size_t>(ng)];
@@ -56,6 +68,9 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       each.verbose = false;
       each.fill_gpu = false;  // the batch's columns fill the GPU together
       each.table_growth = false;  // the batch launches its instances' kernels itself
+      each.table = pool_ + off;
+      each.table_slots = caps[i];
+      off += caps[i];
       inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
     }
     energies_.assign(fcis.size(), 0.0);
@@ -63,6 +78,8 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
     set_groups();
   } catch (...) {
     inst_.clear();
+    if (pool_) cudaFree(pool_);
+    pool_ = nullptr;
     for (size_t g = 0; g < groups_.size(); ++g)
       if (g > 0 && groups_[g].stream) cudaStreamDestroy(groups_[g].stream);
     for (auto e : join_)
@@ -77,6 +94,7 @@ GpuBatch::~GpuBatch() {
     if (groups_[g].graph) cudaGraphExecDestroy(groups_[g].graph);
   }
   inst_.clear();
+  if (pool_) cudaFree(pool_);
   for (size_t g = 1; g < groups_.size(); ++g)
     if (groups_[g].stream) cudaStreamDestroy(groups_[g].stream);
   for (auto e : join_)

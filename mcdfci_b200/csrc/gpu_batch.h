@@ -70,6 +70,7 @@ class GpuBatch {
   long long graph_iters_ = 0;
   std::vector<double> energies_;
   std::vector<char> active_;
+  Slot* pool_ = nullptr;  // every instance's hash table, one allocation
 };
 
 }  // namespace mcd

@@ -271,6 +271,17 @@ void GpuSolver::check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw McdError(MCD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+size_t GpuSolver::full_capacity(const Fcidump& fci, double max_memory) {
+  // Table sizing as run_cdfci_wrapper (src/run_wrapper.h:203-213): the
+  // largest power of two of determinants whose reference footprint
+  // (8*N + 16 bytes, N words per determinant) stays below max_memory.
+  const int n_words = 1 + (fci.norb - 1) / 64;
+  const double bytes_per_det = static_cast<double>(n_words * 8 + 16);
+  size_t pow2 = 8;
+  while (static_cast<double>(pow2) * bytes_per_det < max_memory * 1073741824.0) pow2 *= 2;
+  return pow2 / 2;
+}
+
 GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   // Option validation (read_input, src/run_wrapper.h:89-119, and this build's limits).
   if (opt_.coordinate_pick != MCD_PICK_GCD_GRAD)
@@ -325,10 +336,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   // Table sizing as run_cdfci_wrapper (src/run_wrapper.h:203-213): the
   // largest power of two of determinants whose reference footprint
   // (8*N + 16 bytes) stays below max_memory; max_wavefunction_size is 0.79 of it.
-  const double bytes_per_det = static_cast<double>(n_words_ * 8 + 16);
-  size_t pow2 = 8;
-  while (static_cast<double>(pow2) * bytes_per_det < opt_.max_memory * 1073741824.0) pow2 *= 2;
-  pow2 /= 2;
+  const size_t pow2 = full_capacity(fci, opt_.max_memory);
   max_capacity_ = pow2;
   max_size_ = static_cast<unsigned long long>(0.79 * static_cast<double>(pow2));
   if (max_capacity_ > (1ull << 32))
@@ -366,7 +374,8 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     const double per_chunk = (first_iters * opt_.k + 1.0) * static_cast<double>(entries_);
     size_t c = static_cast<size_t>(1) << 16;
     while (c < max_capacity_ && 0.75 * static_cast<double>(c) < per_chunk) c <<= 1;
-    if (!opt_.table_growth || c >= max_capacity_ || c + max_capacity_ > budget_slots_) c = max_capacity_;
+    if (!opt_.table_growth || opt_.table || c >= max_capacity_ || c + max_capacity_ > budget_slots_)
+      c = max_capacity_;
     capacity_ = c;
   }
   setup_ms_[7] = ms_since(t_dev);
@@ -416,7 +425,15 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     hd_.vss = reinterpret_cast<const double*>(base + o_vss);
     hd_.wab = reinterpret_cast<const double*>(base + o_wab);
 
-    d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
+    if (opt_.table) {
+      if (opt_.table_slots != capacity_)
+        throw McdError(MCD_ERR_INVALID, "the given table has " + std::to_string(opt_.table_slots) +
+                                            " slots; max_memory gives " + std::to_string(capacity_) + ".");
+      d_slots_ = opt_.table;
+      own_table_ = false;
+    } else {
+      d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
+    }
     // The iteration's small buffers in one allocation.
     // Per-CTA partial lists for the largest CTA count the autotuner tries.
     const size_t parts = static_cast<size_t>(opt_.k) * std::max(groups_, opt_.autotune ? kMaxGroups : 1);
@@ -501,7 +518,7 @@ void GpuSolver::release() {
   graph_ = nullptr;
   if (stream_) cudaStreamSynchronize(stream_);
   cudaFree(d_tables_);
-  cudaFree(d_slots_);
+  if (own_table_) cudaFree(d_slots_);
   cudaFree(d_misc_);
   d_misc_ = nullptr;
   d_sect_ = nullptr;

@@ -42,6 +42,10 @@ struct SolverOptions {
   // iterations of the solve) the first time enough iterations are run, and
   // remember the choice per (orbitals, electrons, k, m, SM count).
   bool autotune = false;
+  // A table the caller owns, of exactly the slots max_memory gives
+  // (full_capacity): the solver uses it, never grows or frees it.
+  Slot* table = nullptr;
+  size_t table_slots = 0;
   bool verbose = false;
   cudaStream_t stream = nullptr;
   int device = -1;
@@ -57,6 +61,8 @@ struct McdError : std::runtime_error {
 class GpuSolver {
  public:
   GpuSolver(const Fcidump& fci, const SolverOptions& opt);
+  // Slots of the full table for this FCIDUMP and max_memory (GB).
+  static size_t full_capacity(const Fcidump& fci, double max_memory);
   ~GpuSolver();
   GpuSolver(const GpuSolver&) = delete;
   GpuSolver& operator=(const GpuSolver&) = delete;
@@ -171,6 +177,7 @@ class GpuSolver {
   size_t max_capacity_ = 0;         // hash slots max_memory gives (the reference's table)
   size_t budget_slots_ = 0;         // device memory for two tables at once, in slots
   int growths_ = 0;
+  bool own_table_ = true;
   int groups_rule_ = 1;      // the CTAs per column the fixed rule gives
   bool tuned_ = false;
   std::vector<std::pair<int, double>> tune_trials_;  // (CTAs per column, column kernel us per iteration)

@@ -220,6 +220,9 @@ int mcd_batch_reset(mcd_batch* b);
 int mcd_batch_run_iterations(mcd_batch* b, int64_t n);
 int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, double* column_ms, double* total_ms);
 int mcd_batch_get_report(mcd_batch* b, int32_t instance, mcd_report* r);
+/* mcd_debug_table_sums of one instance: sum x^2 and sum x z over its table
+ * (double-double) and its occupied slots. */
+int mcd_batch_table_sums(mcd_batch* b, int32_t instance, double xx[2], double xz[2], uint64_t* occupied);
 /* mcd_residual of one instance: ||H c - E c|| / ||c|| of its current vector. */
 int mcd_batch_residual(mcd_batch* b, int32_t instance, double* residual);
 /* Energies of the last batch solve, one per instance. */

@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
     "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual", "mcd_debug_scatter_rate_mode",
-    "mcd_debug_autotune_info",
+    "mcd_debug_autotune_info", "mcd_batch_table_sums",
 )
 
 
@@ -170,6 +170,7 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_table_info.argtypes = [vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_setup_times.argtypes = [vp, _dp, ctypes.c_int32]
     L.mcd_batch_residual.argtypes = [vp, ctypes.c_int32, _dp]
+    L.mcd_batch_table_sums.argtypes = [vp, ctypes.c_int32, _dp, _dp, _u64p]
     L.mcd_debug_autotune_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32), _dp, ctypes.c_int32,
                                           ctypes.POINTER(ctypes.c_int32)]
@@ -647,6 +648,12 @@ class CDFCIBatch:
         r = mcd_report()
         _check(library().mcd_batch_get_report(self._h, int(i), ctypes.byref(r)))
         return r.as_dict()
+
+    def table_sums(self, i: int) -> dict:
+        xx, xz = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+        occ = ctypes.c_uint64()
+        _check(library().mcd_batch_table_sums(self._h, int(i), xx, xz, ctypes.byref(occ)))
+        return {"xx": tuple(xx), "xz": tuple(xz), "occupied": occ.value}
 
     def residual(self, i: int) -> float:
         """||H c - E c|| / ||c|| of instance i's current vector."""

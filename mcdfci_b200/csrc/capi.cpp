@@ -322,6 +322,20 @@ int mcd_batch_run_iterations_timed(mcd_batch* b, int64_t n, double* leader_ms, d
   });
 }
 
+int mcd_batch_table_sums(mcd_batch* b, int32_t instance, double xx[2], double xz[2], uint64_t* occupied) {
+  return guarded([&] {
+    if (!b) return fail(MCD_ERR_INVALID, "batch is NULL.");
+    if (instance < 0 || instance >= b->impl->size()) return fail(MCD_ERR_INVALID, "instance out of range.");
+    mcd::dd a, c;
+    unsigned long long n = 0;
+    b->impl->instance(instance).table_sums(&a, &c, &n);
+    if (xx) { xx[0] = a.hi; xx[1] = a.lo; }
+    if (xz) { xz[0] = c.hi; xz[1] = c.lo; }
+    if (occupied) *occupied = n;
+    return MCD_OK;
+  });
+}
+
 int mcd_batch_residual(mcd_batch* b, int32_t instance, double* residual) {
   return guarded([&] {
     if (!b || !residual) return fail(MCD_ERR_INVALID, "NULL argument.");

@@ -58,7 +58,14 @@ def _converge_batch(paths):
         res = [b.residual(i) for i in range(len(paths))]
         if max(res) < RESIDUAL:
             break
-    e = [b.report(i)["energy"] for i in range(len(paths))]
+    # The energy of each final vector from double-double sums over its table
+    # (sum x z / sum x^2), not the solve's running xz, which carries the
+    # rounding of every iteration's update.
+    e = []
+    for i in range(len(paths)):
+        t = b.table_sums(i)
+        e.append(float((np.longdouble(t["xz"][0]) + np.longdouble(t["xz"][1])) /
+                       (np.longdouble(t["xx"][0]) + np.longdouble(t["xx"][1]))))
     b.close()
     return e, res, it
 

@@ -97,12 +97,12 @@ typedef struct mcd_options {
    * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
   int32_t table_growth;
   /* 0 (default): every subspace eigenproblem by the full reduction
-   * (Householder, multisection, inverse iteration).  2: first by shifted
+   * (Householder, multisection, inverse iteration).  1: first by shifted
    * inverse iteration (a Cholesky factorisation of B - sigma I, sigma below
    * the current energy by 16 times the last energy drop, certifies sigma <
    * lambda_1; the current vector starts it), its steps run by one warp on the
-   * explicit inverse, with the full reduction when that fails; 1: the same
-   * with block-wide steps.  On 24 orbitals, k = 32, the shifted solver costs
+   * explicit inverse, with the full reduction when that fails.  On 24
+   * orbitals, k = 32, the shifted solver costs
    * as much as the reduction late in a solve and more early on (it needs
    * more steps while the energy still drops fast), hence the default.  No
    * counterpart in the reference (LAPACK dsyevr, src/solver.h:400-411). */

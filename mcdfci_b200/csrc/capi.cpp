@@ -72,7 +72,7 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.groups = o->groups;
   s.compaction = o->compaction != 0;
   s.table_growth = o->table_growth != 0;
-  if (o->eig_shift < 0 || o->eig_shift > 2) throw mcd::McdError(MCD_ERR_INVALID, "eig_shift must be 0, 1 or 2.");
+  if (o->eig_shift < 0 || o->eig_shift > 1) throw mcd::McdError(MCD_ERR_INVALID, "eig_shift must be 0 or 1.");
   s.eig_shift = o->eig_shift;
   s.autotune = o->autotune != 0;
   s.verbose = o->verbose != 0;

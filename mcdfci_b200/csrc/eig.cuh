@@ -760,10 +760,11 @@ __device__ __forceinline__ void eig_lowest(double* A, int lda, int n, const EigV
 //        false.
 //    (b) L^-1 explicitly, one thread per column, into Li (lower triangle,
 //        zeros above).
-//    (c) Power steps v <- C v / |C v| with C = L^-T L^-1, two triangular
-//        matrix-vector products (no serial chain), until successive vectors
-//        agree to 1e-12 or stop improving; each step divides the other
-//        eigenvectors' share by at least (lambda_2 - sigma)/(lambda_1 - sigma).
+//    (c) Power steps v <- C v / |C v| with C = (A - sigma I)^-1 = L^-T L^-1
+//        formed once, one matrix-vector product per step (no serial chain),
+//        until successive vectors agree to 1e-12 or stop improving; each step
+//        divides the other eigenvectors' share by at least
+//        (lambda_2 - sigma)/(lambda_1 - sigma).
 //    (d) Refinement: C applied to the residual instead of the vector.  With
 //        rho = v'Av and r = A v - rho v, exactly (A - sigma I)^-1 v =
 //        (v - (A - sigma I)^-1 r) / (rho - sigma).  The explicit inverse is
@@ -783,188 +784,6 @@ constexpr int kShiftRefineSteps = 6;
 
 // Per-row values of three rows per lane at most (n <= 96).
 constexpr int kShiftQ = 3;
-
-// Sum over the threads [0, 32*nw) of v; every one of them receives it.
-// part: nw doubles of shared scratch; bar_id: a named barrier of 32*nw threads.
-__device__ __forceinline__ double shift_sum(double v, double* part, int nw, int bar_id) {
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) part[warp] = v;
-  bar_named(bar_id, 32 * nw);
-  double t = 0.0;
-  for (int w = 0; w < nw; ++w) t += part[w];
-  bar_named(bar_id, 32 * nw);
-  return t;
-}
-
-__device__ bool eig_lowest_shifted(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
-                                   int* steps, double* diff, SectionClock& clk) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nw = (n + 31) >> 5;  // warps with a row each
-  __shared__ bool s_ok;
-  __shared__ int s_steps;
-  __shared__ double s_part[4], s_diff;
-  if (tid == 0) {
-    s_ok = true;
-    s_steps = 0;
-    s_diff = 0.0;
-  }
-  for (int i = tid; i < n; i += blockDim.x) V.d[i] = A[i * lda + i];
-  __syncthreads();
-
-  // (a) Cholesky by warp 0.
-  if (warp == 0) {
-    bool ok = true;
-    for (int j = 0; j < n; ++j) {
-      const double* Lj = A + j * lda;
-      double sv[kShiftQ];
-#pragma unroll
-      for (int q = 0; q < kShiftQ; ++q) {
-        const int i = j + lane + 32 * q;
-        sv[q] = 0.0;
-        if (i < n) {
-          const double* Lr = A + i * lda;
-          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-          int c = 0;
-          for (; c + 4 <= j; c += 4) {
-            a0 = fma(Lr[c], Lj[c], a0);
-            a1 = fma(Lr[c + 1], Lj[c + 1], a1);
-            a2 = fma(Lr[c + 2], Lj[c + 2], a2);
-            a3 = fma(Lr[c + 3], Lj[c + 3], a3);
-          }
-          for (; c < j; ++c) a0 = fma(Lr[c], Lj[c], a0);
-          const double aij = (i == j) ? Lr[j] - sigma : Lr[j];
-          sv[q] = aij - ((a0 + a1) + (a2 + a3));
-        }
-      }
-      const double d = __shfl_sync(~0u, sv[0], 0);  // row j is lane 0's first row
-      if (!(d > 0.0)) {
-        ok = false;
-        break;
-      }
-      const double r = rsqrt(d);
-      if (lane == 0) {
-        A[j * lda + j] = d * r;
-        V.ru[j] = r;
-      }
-#pragma unroll
-      for (int q = 0; q < kShiftQ; ++q) {
-        const int i = j + lane + 32 * q;
-        if (i > j && i < n) A[i * lda + j] = sv[q] * r;
-      }
-      __syncwarp();
-    }
-    if (lane == 0 && !ok) s_ok = false;
-  }
-  __syncthreads();
-  clk.mark(17);
-  if (!s_ok) {
-    *steps = 0;
-    *diff = 0.0;
-    return false;
-  }
-
-  // (b) L^-1, column j by thread j.
-  if (tid < n) {
-    const int j = tid;
-    for (int i = 0; i < n; ++i) {
-      const double* Lr = A + i * lda;
-      double a0 = (i == j) ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int c = 0;
-      for (; c + 4 <= i; c += 4) {
-        a0 = fma(-Lr[c], Li[c * lda + j], a0);
-        a1 = fma(-Lr[c + 1], Li[(c + 1) * lda + j], a1);
-        a2 = fma(-Lr[c + 2], Li[(c + 2) * lda + j], a2);
-        a3 = fma(-Lr[c + 3], Li[(c + 3) * lda + j], a3);
-      }
-      for (; c < i; ++c) a0 = fma(-Lr[c], Li[c * lda + j], a0);
-      Li[i * lda + j] = ((a0 + a1) + (a2 + a3)) * V.ru[i];
-    }
-  }
-  __syncthreads();
-  clk.mark(18);
-
-  // (c) Power steps on C = L^-T L^-1 by the first nw warps; the others wait
-  //     at the closing barrier.  v in V.y (normalised first), L^-1 v in V.c.
-  if (warp < nw) {
-    const int i = tid;
-    const bool row = i < n;
-    int nsteps = 0;
-    double last = 0.0;
-    double vi = row ? V.y[i] : 0.0;
-    const double nrm = shift_sum(vi * vi, s_part, nw, 1);
-    vi *= rsqrt(nrm);
-    if (row) V.y[i] = vi;
-    bar_named(1, 32 * nw);
-    double prev = 1e300;
-    bool conv = false;
-    for (int it = 0; it < kShiftPowerSteps && !conv; ++it) {
-      double y = 0.0;
-      if (row)
-        for (int c = 0; c <= i; ++c) y = fma(Li[i * lda + c], V.y[c], y);
-      if (row) V.c[i] = y;
-      bar_named(1, 32 * nw);
-      double w = 0.0;
-      if (row)
-        for (int c = i; c < n; ++c) w = fma(Li[c * lda + i], V.c[c], w);
-      const double ww = shift_sum(w * w, s_part, nw, 1);
-      const double vn = w * rsqrt(ww);
-      const double dd2 = shift_sum((vn - vi) * (vn - vi), s_part, nw, 1);
-      vi = vn;
-      if (row) V.y[i] = vi;
-      bar_named(1, 32 * nw);
-      ++nsteps;
-      const double dv = sqrt(dd2);
-      // converged, or at the rounding floor of the explicit inverse
-      conv = dv < 1e-12 || (dv < 1e-8 && dv > 0.5 * prev);
-      prev = dv;
-    }
-    clk.mark(19);
-    // (d) Refinement steps: w = v - C r, r = A v - rho v.
-    bool done = false;
-    for (int it = 0; it < kShiftRefineSteps && !done; ++it) {
-      double av = 0.0;
-      if (row) {
-        for (int c = 0; c < n; ++c) {
-          const double aic = (c == i) ? V.d[i] : (c > i ? A[i * lda + c] : A[c * lda + i]);
-          av = fma(aic, V.y[c], av);
-        }
-      }
-      const double rho = shift_sum(vi * av, s_part, nw, 1);
-      const double r = av - rho * vi;
-      if (row) V.g[i] = r;
-      bar_named(1, 32 * nw);
-      double y = 0.0;
-      if (row)
-        for (int c = 0; c <= i; ++c) y = fma(Li[i * lda + c], V.g[c], y);
-      if (row) V.c[i] = y;
-      bar_named(1, 32 * nw);
-      double t = 0.0;
-      if (row)
-        for (int c = i; c < n; ++c) t = fma(Li[c * lda + i], V.c[c], t);
-      const double w = vi - t;
-      const double ww = shift_sum(w * w, s_part, nw, 1);
-      const double vn = w * rsqrt(ww);
-      const double dd2 = shift_sum((vn - vi) * (vn - vi), s_part, nw, 1);
-      vi = vn;
-      if (row) V.y[i] = vi;
-      bar_named(1, 32 * nw);
-      ++nsteps;
-      last = sqrt(dd2);
-      done = last < 2e-15 * sqrt(static_cast<double>(n));
-    }
-    if (tid == 0) {
-      s_ok = done;
-      s_steps = nsteps;
-      s_diff = last;
-    }
-  }
-  __syncthreads();
-  clk.mark(20);
-  *steps = s_steps;
-  *diff = s_diff;
-  return s_ok;
-}
 
 // (a) and (b) with the matrix in registers, for n <= kShiftRegRows: 160
 // threads, row r = t/4 held by four lanes, lane quarter q keeping columns
@@ -1059,12 +878,12 @@ __device__ bool shift_factor_reg(double* A, int lda, int n, double sigma, const 
   return true;
 }
 
-// The same method with (c) and (d) run by one warp on the explicit
-// C = L^-T L^-1 (formed once by the whole block into Ci): each power step
-// is one matrix-vector product with up to kShiftQ rows per lane and two
-// shuffle reductions, with no block barrier; each refinement step adds the
-// residual's product with A (upper triangle and V.d).  (a) and (b) as in
-// eig_lowest_shifted.  Same contract, plus Ci: n x lda shared doubles.
+// The shifted solver: (a) and (b) in registers up to kShiftRegRows rows
+// (shift_factor_reg), else by one warp in shared memory (a Crout Cholesky,
+// then L^-1 one column per thread); C formed by the whole block into Ci
+// (n x lda shared doubles); (c) and (d) by one warp, up to kShiftQ rows per
+// lane, shuffle reductions and no block barrier, each refinement step
+// adding the residual's product with A (upper triangle and V.d).
 __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
                                         double* Ci, int* steps, double* diff, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

@@ -34,9 +34,8 @@ struct SolverOptions {
   // allocation) as it fills, up to the size max_memory gives; false: the
   // whole table is allocated at creation, as the reference reserves it.
   bool table_growth = true;
-  // Subspace eigenproblem: 0 the full reduction every time; 2 shifted
-  // inverse iteration first, its steps by one warp on the explicit inverse;
-  // 1 the same with block-wide steps.
+  // Subspace eigenproblem: 0 the full reduction every time; 1 shifted
+  // inverse iteration first, with the reduction when it fails.
   int eig_shift = 0;
   // Choose the CTAs per Hamiltonian column from timed trials (real
   // iterations of the solve) the first time enough iterations are run, and

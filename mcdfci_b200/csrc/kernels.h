@@ -103,8 +103,7 @@ struct LeaderLaunch {
   unsigned long long* sect;  // [kLeaderSections] SM cycles per phase of the leader kernel, or null
   int m;
   int k_req;
-  int eig_shift;          // shifted inverse iteration first when the last energy drop is known:
-                          // 0 never, 1 block-wide steps, 2 one-warp steps on the explicit inverse
+  int eig_shift;          // 1: shifted inverse iteration first when the last energy drop is known
 };
 
 // Several independent instances advanced by the same two launches per

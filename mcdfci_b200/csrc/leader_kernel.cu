@@ -180,10 +180,8 @@ __host__ __device__ constexpr size_t eig_work_doubles(int k) {
 // its Rayleigh quotient there is xz/xx) and the current vector as the start;
 // the reduction runs when that fails or its residual is not below 1e-11
 // (1 + |lambda|).
-// method: 1 the block-wide steps (eig_lowest_shifted), 2 the one-warp steps
-// on the explicit inverse (eig_lowest_shifted_warp).
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
-                                double* dx, double* work, SectionClock& clk, double drop, int method = 2) {
+                                double* dx, double* work, SectionClock& clk, double drop) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1, s_res;
   __shared__ int s_branch;
@@ -289,8 +287,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     __syncthreads();
     int steps = 0;
     double diff = 0.0;
-    shifted = method == 1 ? eig_lowest_shifted(A, lda, n, V, e_cur - delta, Li, &steps, &diff, clk)
-                          : eig_lowest_shifted_warp(A, lda, n, V, e_cur - delta, Li, Ci, &steps, &diff, clk);
+    shifted = eig_lowest_shifted_warp(A, lda, n, V, e_cur - delta, Li, Ci, &steps, &diff, clk);
     res.shift_steps = shifted ? steps : 0;
     res.shift_diff = shifted ? diff : 0.0;
     if (!shifted) {
@@ -854,7 +851,7 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
 
   // 6. Eig update.
   const EigResult er =
-      eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0, L.eig_shift);
+      eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0);
   clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {

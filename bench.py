@@ -481,15 +481,20 @@ def autotune_object(mc, tmp, args, local_rank):
     from mcdfci_b200 import synth
 
     out = {}
-    for name, k, mem, zt in (("n24_6a6b", 32, 8.0, 1e-9), ("n16_5a5b", 16, 1.0, 0.0), ("n42_24a24b", 64, 32.0, 1e-6)):
+    for name, k, mem, zt in (("n24_6a6b", 32, 8.0, 1e-9), ("n16_5a5b", 16, 1.0, 0.0), ("n42_24a24b", 64, 100.0, 1e-5)):
         p = os.path.join(tmp, f"tune_{name}.fcidump")
         synth.write_fcidump(p, name, seed=args.seed)
         s = mc.CDFCI(mc.Fcidump(p), num_of_coordinate=k, estimate=k, max_memory=mem, z_threshold=zt, threshold=0.0,
                      device=local_rank, autotune=True, num_iterations=256)
-        s.reset()
-        s.run_iterations(16 * 10)
-        info = s.autotune_info()
-        s.close()
+        try:
+            s.reset()
+            s.run_iterations(16 * 10)
+            info = s.autotune_info()
+        except mc.McdError as e:
+            out[name] = {"k": k, "error": str(e)}
+            continue
+        finally:
+            s.close()
         rule_us = next((t["column_us"] for t in info["trials"] if t["groups"] == info["rule"]), None)
         best_us = min((t["column_us"] for t in info["trials"]), default=None)
         out[name] = {"k": k, "rule_groups": info["rule"], "chosen_groups": info["chosen"],

@@ -748,6 +748,9 @@ long long GpuSolver::autotune_groups(long long budget) {
     }
   }
   set_groups(best);
+  // A trial that ended in a device error (a full table, say) timed no work:
+  // surface the error instead of keeping its choice.
+  read_state();
   std::lock_guard<std::mutex> lock(g_tune_mu);
   g_tune_cache[key] = best;
   return done;

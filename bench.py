@@ -755,6 +755,17 @@ def e2e_run(mc, fc, args, local_rank):
 
     iters = args.steps
     interval = max(1, iters // 10)
+    # Warm-up: one small solve through the same calls (7 orbitals, the same
+    # k and m), so that the clock below sees a process whose kernels are
+    # loaded, as the warm-up steps precede the device-timed value.
+    from mcdfci_b200 import synth
+
+    wpath = os.path.join(os.path.dirname(fc.path), "warmup_n7.fcidump")
+    synth.write_fcidump(wpath, "n7_5a5b", seed=0)
+    w = mc.CDFCI(mc.Fcidump(wpath), num_of_coordinate=args.k, estimate=args.m, max_memory=0.001,
+                 threshold=0.0, device=local_rank, num_iterations=10, report_interval=5)
+    w.solve()
+    w.close()
     t0 = time.perf_counter()
     s = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                  z_threshold=args.z_threshold, threshold=0.0, device=local_rank, num_iterations=iters,
@@ -792,7 +803,8 @@ def e2e_run(mc, fc, args, local_rank):
             "stages": breakdown,
             "what": "mcd_create_from_fcidump (Hamiltonian tables host->device, hash table allocation) + mcd_solve "
                     f"(table fill, {iters} iterations, a report read back every {interval}) + mcd_result; "
-                    "mcd_destroy after the clock"}
+                    "mcd_destroy after the clock; after one 10-iteration warm-up solve of a 7-orbital problem "
+                    "in the same process (kernels loaded)"}
 
 
 def main():

@@ -22,8 +22,33 @@
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 namespace mcd {
+
+namespace {
+
+// f(i) for i in [0, n) on up to 16 host threads (each a contiguous range);
+// every i writes its own part of the tables, so no two threads share one.
+template <typename F>
+void parallel_for(int n, F f) {
+  const int hw = static_cast<int>(std::thread::hardware_concurrency());
+  const int nt = std::max(1, std::min({n, hw > 0 ? hw : 1, 16}));
+  if (nt <= 1) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (int i = n * t / nt; i < n * (t + 1) / nt; ++i) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
 
 HamHost build_hamiltonian(const Fcidump& fci, double thr) {
   if (!(thr >= 0.0)) throw std::invalid_argument("hamiltonian:threshold must be >= 0.");
@@ -87,9 +112,10 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
   // Same-spin doubles.
   const size_t np = static_cast<size_t>(h.npair);
   h.vss.assign(2 * np * np, 0.0);
-  for (int s = 0; s < 2; ++s)
-    for (int q = 1; q < n; ++q)
-      for (int p = 0; p < q; ++p) {
+  parallel_for(2 * n, [&](int sq) {
+    const int s = sq / n, q = sq % n;
+    if (q == 0) return;
+    for (int p = 0; p < q; ++p) {
         const int i = 2 * p + s, j = 2 * q + s;
         for (int ss = 1; ss < n; ++ss)
           for (int r = 0; r < ss; ++r) {
@@ -97,11 +123,12 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
             const double v = fci.g(i, j, a, b) - fci.g(i, j, b, a);
             if (std::fabs(v) > thr) h.vss[(s * np + pair_index(p, q)) * np + pair_index(r, ss)] = v;
           }
-      }
+    }
+  });
 
   // Opposite-spin doubles.
   h.wab.assign(static_cast<size_t>(n) * n * n * n, 0.0);
-  for (int pa = 0; pa < n; ++pa)
+  parallel_for(n, [&](int pa) {
     for (int pb = 0; pb < n; ++pb)
       for (int ra = 0; ra < n; ++ra)
         for (int sb = 0; sb < n; ++sb) {
@@ -112,6 +139,7 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
             v = fci.g(2 * pb + 1, 2 * pa, 2 * sb + 1, 2 * ra);
           if (std::fabs(v) > thr) h.wab[((static_cast<size_t>(pa) * n + pb) * n + ra) * n + sb] = v;
         }
+  });
   (void)sp;
   return h;
 }

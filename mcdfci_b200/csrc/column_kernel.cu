@@ -313,8 +313,7 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
         // (the diagonal entry's slot is the picked determinant's own).
         const uint64_t home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
         uint64_t ka = 0, kb = 0;
-        double hx = 0.0, hz = 0.0;
-        load_slot(L.tab.slots + home, ka, kb, hx, hz);
+        load_key(L.tab.slots + home, ka, kb);
         long long q1 = 0;
         if (timed) {
           q1 = clock64();
@@ -334,26 +333,8 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
           }
           if (slot >= 0) {
             Slot* sp = L.tab.slots + slot;
-            // x and z as loaded with the key when the home slot holds the
-            // determinant (the usual case), else read now; z is then added
-            // to without a return (a reduction: no second round trip), and
-            // the candidate score uses the loaded z plus dz.  The adds of
-            // other columns to the same slot in between are missed by the
-            // score only, as they are by the reference's threads; the
-            // leader re-reads every candidate's (x, z) before it picks.
-            double x, z0;
-            if (inserted) {
-              x = 0.0;
-              z0 = 0.0;
-            } else if (slot == static_cast<long long>(home)) {
-              x = hx;
-              z0 = hz;
-            } else {
-              x = load_relaxed(&sp->x);
-              z0 = load_relaxed(&sp->z);
-            }
-            atomicAdd(&sp->z, dz);
-            const double znew = z0 + dz;
+            const double x = sp->x;
+            const double znew = atomicAdd(&sp->z, dz) + dz;
             ++upd;
             acc_newz += v * x;
             acc_dot += dz * x;

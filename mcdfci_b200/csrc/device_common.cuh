@@ -130,22 +130,6 @@ __device__ __forceinline__ void cas_key(Slot* s, uint64_t na, uint64_t nb, uint6
       : "l"(ea), "l"(eb), "l"(na), "l"(nb), "l"(s)
       : "memory");
 }
-// The whole 32-byte slot: the key and (x, z), two 128-bit relaxed loads
-// issued together (one sector).
-__device__ __forceinline__ void load_slot(const Slot* s, uint64_t& a, uint64_t& b, double& x, double& z) {
-  uint64_t xb, zb;
-  asm volatile(
-      "{\n\t.reg .b128 d, e;\n\t"
-      "ld.relaxed.gpu.global.b128 d, [%4];\n\t"
-      "ld.relaxed.gpu.global.b128 e, [%4+16];\n\t"
-      "mov.b128 {%0, %1}, d;\n\t"
-      "mov.b128 {%2, %3}, e;\n\t}"
-      : "=l"(a), "=l"(b), "=l"(xb), "=l"(zb)
-      : "l"(s)
-      : "memory");
-  x = __longlong_as_double(static_cast<long long>(xb));
-  z = __longlong_as_double(static_cast<long long>(zb));
-}
 __device__ __forceinline__ double load_relaxed(const double* p) {
   double v;
   asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");

@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <future>
 #include <iomanip>
 #include <iostream>
 #include <map>
@@ -310,21 +312,48 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
 
   using clock = std::chrono::steady_clock;
   auto ms_since = [](clock::time_point t) { return std::chrono::duration<double, std::milli>(clock::now() - t).count(); };
-  auto t_host = clock::now();
-  try {
-    ham_ = build_hamiltonian(fci, opt_.threshold);
-    std::string warning;
-    if (opt_.ref_det_occ.empty()) {
-      ref_ = hartree_fock(fci, &warning);
-      if (!warning.empty() && opt_.verbose) std::cout << warning << std::endl << std::endl;
-    } else {
-      ref_ = ref_det_from_occ(fci, opt_.ref_det_occ);
+  // The host tables are built on a host thread while this one sets up the
+  // device and allocates; they are joined before the upload.  Errors keep
+  // the order of a serial build: the tables' own checks first, then the
+  // reference determinant's.
+  double host_ms = 0.0;
+  std::future<HamHost> host = std::async(std::launch::async, [&fci, &host_ms, thr = opt_.threshold] {
+    const auto t = std::chrono::steady_clock::now();
+    HamHost h = build_hamiltonian(fci, thr);
+    host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+    return h;
+  });
+  auto join_host = [&] {
+    try {
+      ham_ = host.get();
+    } catch (const std::invalid_argument& e) {
+      throw McdError(MCD_ERR_INVALID, e.what());
     }
-  } catch (const std::invalid_argument& e) {
-    throw McdError(MCD_ERR_INVALID, e.what());
+    setup_ms_[0] = host_ms;
+  };
+  {
+    std::exception_ptr ref_err;
+    try {
+      std::string warning;
+      if (opt_.ref_det_occ.empty()) {
+        ref_ = hartree_fock(fci, &warning);
+        if (!warning.empty() && opt_.verbose) std::cout << warning << std::endl << std::endl;
+      } else {
+        ref_ = ref_det_from_occ(fci, opt_.ref_det_occ);
+      }
+    } catch (const std::invalid_argument&) {
+      ref_err = std::current_exception();
+    }
+    // Inputs that the tables reject end here, before any device work.
+    if (ref_err || fci.norb % 2 || !(opt_.threshold >= 0.0)) {
+      join_host();
+      try {
+        std::rethrow_exception(ref_err);
+      } catch (const std::invalid_argument& e) {
+        throw McdError(MCD_ERR_INVALID, e.what());
+      }
+    }
   }
-  ref_diag_ = diagonal_element(ham_, ref_);
-  setup_ms_[0] = ms_since(t_host);
   na_ = __builtin_popcountll(ref_.a);
   nb_ = __builtin_popcountll(ref_.b);
   if (na_ >= 64)  // its only determinant would carry the empty-slot key
@@ -381,11 +410,15 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   setup_ms_[7] = ms_since(t_dev);
 
   auto t_alloc = clock::now();
-  double upload_ms = 0.0;
+  auto t_join = t_alloc;
+  double alloc_ms = 0.0;
   try {
-    // Hamiltonian tables in one allocation.
-    const size_t n_hd = ham_.hdiag.size(), n_d2 = ham_.d2.size(), n_sh = ham_.sh.size(), n_st = ham_.st.size(),
-                 n_sp = ham_.spres.size(), n_vss = ham_.vss.size(), n_wab = ham_.wab.size();
+    // Hamiltonian tables in one allocation, sized from the orbital count
+    // while the host tables are still being built.
+    const size_t no = static_cast<size_t>(fci.norb / 2), nso = static_cast<size_t>(fci.norb);
+    const size_t npr = no * (no - 1) / 2;
+    const size_t n_hd = nso, n_d2 = nso * nso, n_sh = 2 * no * no, n_st = 2 * no * no * nso, n_sp = 2 * no,
+                 n_vss = 2 * npr * npr, n_wab = no * no * no * no;
     size_t off = 0;
     const size_t o_hd = off;
     off = align_up(off + n_hd * 8, 256);
@@ -406,17 +439,10 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     auto up = [&](size_t o, const void* src, size_t bytes) {
       if (bytes) check(cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, stream_), "upload tables");
     };
-    up(o_hd, ham_.hdiag.data(), n_hd * 8);
-    up(o_d2, ham_.d2.data(), n_d2 * 8);
-    up(o_sh, ham_.sh.data(), n_sh * 8);
-    up(o_st, ham_.st.data(), n_st * 8);
-    up(o_sp, ham_.spres.data(), n_sp * 8);
-    up(o_vss, ham_.vss.data(), n_vss * 8);
-    up(o_wab, ham_.wab.data(), n_wab * 8);
-    hd_.norb = ham_.norb;
-    hd_.nso = ham_.nso;
-    hd_.npair = ham_.npair;
-    hd_.ecore = ham_.ecore;
+    hd_.norb = static_cast<int>(no);
+    hd_.nso = static_cast<int>(nso);
+    hd_.npair = static_cast<int>(npr);
+    hd_.ecore = fci.core_energy;
     hd_.hdiag = reinterpret_cast<const double*>(base + o_hd);
     hd_.d2 = reinterpret_cast<const double*>(base + o_d2);
     hd_.sh = reinterpret_cast<const double*>(base + o_sh);
@@ -468,6 +494,22 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     check(cudaMemsetAsync(d_done_, 0, kMaxK * sizeof(unsigned), stream_), "memset");
     h_occ_ = pinned_words_acquire();
     for (auto& e : ev_occ_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+
+    // The host tables, then their upload.
+    alloc_ms = ms_since(t_alloc);
+    t_join = clock::now();
+    join_host();
+    ref_diag_ = diagonal_element(ham_, ref_);
+    if (ham_.hdiag.size() != n_hd || ham_.d2.size() != n_d2 || ham_.sh.size() != n_sh || ham_.st.size() != n_st ||
+        ham_.spres.size() != n_sp || ham_.vss.size() != n_vss || ham_.wab.size() != n_wab)
+      throw std::logic_error("host table sizes differ from the device allocation.");
+    up(o_hd, ham_.hdiag.data(), n_hd * 8);
+    up(o_d2, ham_.d2.data(), n_d2 * 8);
+    up(o_sh, ham_.sh.data(), n_sh * 8);
+    up(o_st, ham_.st.data(), n_st * 8);
+    up(o_sp, ham_.spres.data(), n_sp * 8);
+    up(o_vss, ham_.vss.data(), n_vss * 8);
+    up(o_wab, ham_.wab.data(), n_wab * 8);
   } catch (...) {
     release();
     throw;
@@ -504,11 +546,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
   ll_.eig_shift = opt_.eig_shift;
-  const auto t_up = clock::now();
   check(cudaStreamSynchronize(stream_), "table upload");
-  upload_ms = ms_since(t_up);
-  setup_ms_[1] = ms_since(t_alloc) - upload_ms;
-  setup_ms_[2] = upload_ms;
+  setup_ms_[1] = alloc_ms;
+  setup_ms_[2] = ms_since(t_join);
 }
 
 GpuSolver::~GpuSolver() { release(); }

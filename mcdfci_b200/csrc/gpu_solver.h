@@ -125,8 +125,9 @@ class GpuSolver {
   long long table_max_capacity() const { return static_cast<long long>(max_capacity_); }
   int table_growths() const { return growths_; }
   // Host wall time of the set-up stages, in milliseconds (kSetupStages values):
-  // 0 Hamiltonian tables and reference determinant on the host, 1 device
-  // allocations of the constructor, 2 table upload, 3 table fill of the last
+  // 0 Hamiltonian tables on the host (built on a host thread during 7 and 1),
+  // 1 device allocations of the constructor, 2 the wait for the host tables
+  // after 1 and their upload, 3 table fill of the last
   // reset (synchronised), 4 CUDA graph builds, 5 table growths, 6 report
   // read-backs (finish, state copy, synchronisation), 7 device and stream
   // set-up (device, stream, attributes, free memory), summed since creation.

@@ -20,6 +20,7 @@
 #include "hamiltonian.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <stdexcept>
 #include <thread>
@@ -29,22 +30,21 @@ namespace mcd {
 
 namespace {
 
-// f(i) for i in [0, n) on up to 16 host threads (each a contiguous range);
-// every i writes its own part of the tables, so no two threads share one.
+// f(i) for every i in [0, n) on up to 16 host threads, each taking the next
+// unclaimed i from a shared counter (the tasks differ in cost); every i
+// writes its own part of the tables, so no two threads share one.
 template <typename F>
-void parallel_for(int n, F f) {
+void parallel_tasks(int n, F f) {
   const int hw = static_cast<int>(std::thread::hardware_concurrency());
   const int nt = std::max(1, std::min({n, hw > 0 ? hw : 1, 16}));
-  if (nt <= 1) {
-    for (int i = 0; i < n; ++i) f(i);
-    return;
-  }
+  std::atomic<int> next{0};
+  auto worker = [&] {
+    for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) f(i);
+  };
   std::vector<std::thread> th;
-  th.reserve(nt);
-  for (int t = 0; t < nt; ++t)
-    th.emplace_back([&, t] {
-      for (int i = n * t / nt; i < n * (t + 1) / nt; ++i) f(i);
-    });
+  th.reserve(nt - 1);
+  for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+  worker();
   for (auto& x : th) x.join();
 }
 
@@ -85,60 +85,71 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
   for (int i = 0; i < nso; ++i)
     for (int j = i + 1; j < nso; ++j) h.d2[i * nso + j] = fci.g(i, j, i, j) - fci.g(i, j, j, i);
 
-  // Singles.
+  // Singles, same-spin and opposite-spin doubles: one pool of tasks, the
+  // most expensive (opposite-spin rows) first.
+  const size_t np = static_cast<size_t>(h.npair);
   h.sh.assign(2 * static_cast<size_t>(n) * n, 0.0);
   h.st.assign(2 * static_cast<size_t>(n) * n * nso, 0.0);
   h.spres.assign(2 * static_cast<size_t>(n), 0);
-  for (int s = 0; s < 2; ++s)
-    for (int p = 0; p < n; ++p)
-      for (int r = 0; r < n; ++r) {
-        const int i = 2 * p + s, a = 2 * r + s;
-        const double one = fci.h(i, a);
-        double maxv = std::fabs(one);
-        double* t = &h.st[((static_cast<size_t>(s) * n + p) * n + r) * nso];
-        for (int k = 0; k < nso; ++k) {
-          double v;
-          if (i <= k)
-            v = fci.g(i, k, a, k) - fci.g(i, k, k, a);
-          else
-            v = fci.g(k, i, k, a) - fci.g(k, i, a, k);
-          t[k] = v;
-          maxv = std::max(maxv, std::fabs(v));
-        }
-        h.sh[(static_cast<size_t>(s) * n + p) * n + r] = one;
-        if (maxv > thr) h.spres[s * n + p] |= 1ull << r;
-      }
-
-  // Same-spin doubles.
-  const size_t np = static_cast<size_t>(h.npair);
   h.vss.assign(2 * np * np, 0.0);
-  parallel_for(2 * n, [&](int sq) {
-    const int s = sq / n, q = sq % n;
-    if (q == 0) return;
-    for (int p = 0; p < q; ++p) {
-        const int i = 2 * p + s, j = 2 * q + s;
-        for (int ss = 1; ss < n; ++ss)
-          for (int r = 0; r < ss; ++r) {
-            const int a = 2 * r + s, b = 2 * ss + s;
-            const double v = fci.g(i, j, a, b) - fci.g(i, j, b, a);
-            if (std::fabs(v) > thr) h.vss[(s * np + pair_index(p, q)) * np + pair_index(r, ss)] = v;
-          }
-    }
-  });
-
-  // Opposite-spin doubles.
   h.wab.assign(static_cast<size_t>(n) * n * n * n, 0.0);
-  parallel_for(n, [&](int pa) {
-    for (int pb = 0; pb < n; ++pb)
-      for (int ra = 0; ra < n; ++ra)
-        for (int sb = 0; sb < n; ++sb) {
-          double v;
-          if (pa <= pb)  // alpha pa (2pa) precedes beta pb (2pb+1)
-            v = fci.g(2 * pa, 2 * pb + 1, 2 * ra, 2 * sb + 1);
-          else
-            v = fci.g(2 * pb + 1, 2 * pa, 2 * sb + 1, 2 * ra);
-          if (std::fabs(v) > thr) h.wab[((static_cast<size_t>(pa) * n + pb) * n + ra) * n + sb] = v;
+  // Single excitations p -> r of spin s, every r.
+  auto singles = [&](int s, int p) {
+    uint64_t pres = 0;
+    for (int r = 0; r < n; ++r) {
+      const int i = 2 * p + s, a = 2 * r + s;
+      const double one = fci.h(i, a);
+      double maxv = std::fabs(one);
+      double* t = &h.st[((static_cast<size_t>(s) * n + p) * n + r) * nso];
+      for (int k = 0; k < nso; ++k) {
+        double v;
+        if (i <= k)
+          v = fci.g(i, k, a, k) - fci.g(i, k, k, a);
+        else
+          v = fci.g(k, i, k, a) - fci.g(k, i, a, k);
+        t[k] = v;
+        maxv = std::max(maxv, std::fabs(v));
+      }
+      h.sh[(static_cast<size_t>(s) * n + p) * n + r] = one;
+      if (maxv > thr) pres |= 1ull << r;
+    }
+    h.spres[s * n + p] = pres;
+  };
+  // Same-spin doubles out of the pairs (p, q), p < q, of spin s.
+  auto same_spin = [&](int s, int q) {
+    for (int p = 0; p < q; ++p) {
+      const int i = 2 * p + s, j = 2 * q + s;
+      for (int ss = 1; ss < n; ++ss)
+        for (int r = 0; r < ss; ++r) {
+          const int a = 2 * r + s, b = 2 * ss + s;
+          const double v = fci.g(i, j, a, b) - fci.g(i, j, b, a);
+          if (std::fabs(v) > thr) h.vss[(s * np + pair_index(p, q)) * np + pair_index(r, ss)] = v;
         }
+    }
+  };
+  // Opposite-spin doubles out of alpha pa and beta pb.
+  auto opposite_spin = [&](int pa, int pb) {
+    for (int ra = 0; ra < n; ++ra)
+      for (int sb = 0; sb < n; ++sb) {
+        double v;
+        if (pa <= pb)  // alpha pa (2pa) precedes beta pb (2pb+1)
+          v = fci.g(2 * pa, 2 * pb + 1, 2 * ra, 2 * sb + 1);
+        else
+          v = fci.g(2 * pb + 1, 2 * pa, 2 * sb + 1, 2 * ra);
+        if (std::fabs(v) > thr) h.wab[((static_cast<size_t>(pa) * n + pb) * n + ra) * n + sb] = v;
+      }
+  };
+  const int n_ab = n * n, n_ss = 2 * n, n_s = 2 * n;
+  parallel_tasks(n_ab + n_ss + n_s, [&](int t) {
+    if (t < n_ab) {
+      opposite_spin(t / n, t % n);
+    } else if (t < n_ab + n_ss) {
+      const int u = t - n_ab;
+      same_spin(u / n, n - 1 - u % n);  // larger q (more pairs) first
+    } else {
+      const int u = t - n_ab - n_ss;
+      singles(u / n, u % n);
+    }
   });
   (void)sp;
   return h;

@@ -1,7 +1,11 @@
 #include "gpu_batch.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <exception>
+#include <thread>
+#include <vector>
 #include <cstdio>
 #include <iomanip>
 #include <iostream>
@@ -59,20 +63,45 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       throw McdError(MCD_ERR_CUDA, "cudaMalloc(batch tables, " + std::to_string(total * sizeof(Slot)) +
                                        " bytes): " + cudaGetErrorString(ae));
     pool_ = static_cast<Slot*>(pool);
+    // Instance i goes to group i % ng, on that group's stream.  The
+    // instances are independent, so they are constructed on up to eight host
+    // threads (host tables, uploads); the device is named explicitly because
+    // each thread has its own current device.  The first failure in instance
+    // order is the one reported.
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    const size_t n = fcis.size();
+    std::vector<SolverOptions> each(n, opt_);
     size_t off = 0;
-    // Instance i goes to group i % ng, on that group's stream.
-    for (size_t i = 0; i < fcis.size(); ++i) {
-      Group& G = groups_[i % static_cast<size_t>(ng)];
-      SolverOptions each = opt_;
-      each.stream = G.stream;
-      each.verbose = false;
-      each.fill_gpu = false;  // the batch's columns fill the GPU together
-      each.table_growth = false;  // the batch launches its instances' kernels itself
-      each.table = pool_ + off;
-      each.table_slots = caps[i];
+    for (size_t i = 0; i < n; ++i) {
+      each[i].device = dev;
+      each[i].stream = groups_[i % static_cast<size_t>(ng)].stream;
+      each[i].verbose = false;
+      each[i].fill_gpu = false;      // the batch's columns fill the GPU together
+      each[i].table_growth = false;  // the batch launches its instances' kernels itself
+      each[i].table = pool_ + off;
+      each[i].table_slots = caps[i];
       off += caps[i];
-      inst_.push_back(std::make_unique<GpuSolver>(*fcis[i], each));
     }
+    inst_.resize(n);
+    std::vector<std::exception_ptr> errs(n);
+    std::atomic<size_t> next{0};
+    auto build = [&] {
+      for (size_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
+        try {
+          inst_[i] = std::make_unique<GpuSolver>(*fcis[i], each[i]);
+        } catch (...) {
+          errs[i] = std::current_exception();
+        }
+      }
+    };
+    const size_t nt = std::min<size_t>(n, 8);
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(build);
+    build();
+    for (auto& x : th) x.join();
+    for (const auto& e : errs)
+      if (e) std::rethrow_exception(e);
     energies_.assign(fcis.size(), 0.0);
     active_.assign(fcis.size(), 1);
     set_groups();

@@ -11,10 +11,15 @@ same with oracle/_ref/cdfci_omp (the reference compiled from its sources by
     python tests/golden/make_curve.py [--iterations 60000] [--jobs 2] [--threads 4]
 
 Deck per point: gcd_grad, eig, num_of_coordinate = estimate = 16 (the
-reference lowers k to its host's core count; the effective k is recorded),
-max_memory 1 GB, z_threshold 0, hamiltonian threshold 0, report every 5000
-iterations.  Output: curve_energies.json, one record per point with t, the
-effective k, the iterations, the energy of every report and the last one.
+reference lowers k to its host's processor count; the effective k is
+recorded), max_memory 1 GB, z_threshold 0, hamiltonian threshold 0, report
+every 1000 iterations.  Output: curve_energies.json, one record per point with
+t, the effective k, the iterations, the energy of every report and the last
+one.  On some points the reference stops before its last iteration: its
+inverse-iteration refinement prints "Factorization fails!" and exits with
+status 255 (src/solver.h:444-450).  Such a point is recorded with
+"failed" (the message and the exit status), the reports it printed, and
+"energy" = its last reported energy (null when it printed none).
 Points are written as they finish, so an interrupted run keeps what it did;
 a rerun skips the points already recorded with the same settings.
 """
@@ -52,7 +57,13 @@ def run_point(i, iterations, threads, report):
                                             "coordinate_pick": "gcd_grad", "coordinate_update": "eig",
                                             "num_of_coordinate": 16, "estimate": 16}}}, f)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
-        res = subprocess.run([CDFCI, deck], capture_output=True, text=True, env=env, check=True)
+        res = subprocess.run([CDFCI, deck], capture_output=True, text=True, env=env)
+    failed = None
+    if res.returncode != 0:
+        msg = [ln.strip() for ln in (res.stdout + res.stderr).splitlines() if "fail" in ln.lower()]
+        if not msg:
+            raise RuntimeError(f"point {i}: the reference exited with status {res.returncode}:\n{res.stdout[-2000:]}")
+        failed = {"message": msg[-1], "exit_status": res.returncode}
     k_eff = 16
     m = re.search(r"Not enough processes\. Set k = (\d+)", res.stdout)
     if m:
@@ -63,14 +74,17 @@ def run_point(i, iterations, threads, report):
         if len(p) >= 9 and re.match(r"^\d+$", p[0]) and re.match(r"^-?\d+\.\d+$", p[1]):
             reports.append({"iteration": int(p[0]), "energy": float(p[1]), "z_size": int(p[4]),
                             "time_s": float(p[7])})
-    return {"point": i, "t": t, "k": k_eff, "iterations": iterations, "reports": reports,
-            "energy": reports[-1]["energy"]}
+    rec = {"point": i, "t": t, "k": k_eff, "iterations": iterations, "report_interval": report, "reports": reports,
+           "energy": reports[-1]["energy"] if reports else None}
+    if failed:
+        rec["failed"] = failed
+    return rec
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iterations", type=int, default=60000)
-    ap.add_argument("--report", type=int, default=5000)
+    ap.add_argument("--report", type=int, default=1000)
     ap.add_argument("--jobs", type=int, default=2)
     ap.add_argument("--threads", type=int, default=4)
     ap.add_argument("--points", type=int, nargs="*", default=list(range(POINTS)))
@@ -84,7 +98,10 @@ def main():
     if os.path.exists(OUT):
         with open(OUT) as f:
             data = json.load(f)
-    done = {p["point"] for p in data["points"] if p["iterations"] == args.iterations}
+    data["deck"]["report_interval"] = args.report
+    data["points"] = [p for p in data["points"]
+                      if p["iterations"] == args.iterations and p.get("report_interval") == args.report]
+    done = {p["point"] for p in data["points"]}
     todo = [i for i in args.points if i not in done]
 
     def save():
@@ -99,7 +116,8 @@ def main():
             rec = fu.result()
             data["points"] = [p for p in data["points"] if p["point"] != rec["point"]] + [rec]
             save()
-            print(json.dumps({"point": rec["point"], "energy": rec["energy"], "k": rec["k"]}), flush=True)
+            print(json.dumps({"point": rec["point"], "energy": rec["energy"], "k": rec["k"],
+                              "failed": rec.get("failed")}), flush=True)
     save()
 
 

@@ -4,10 +4,14 @@ tests/golden/curve_energies.json holds, for each of the 32 points (16
 orbitals, 5 + 5 electrons, mcdfci_b200.synth "n16_5a5b" at t = i/31), the
 energy the reference (its solver compiled from its sources,
 tests/golden/make_curve.py) reached after its iterations, with its report
-history.  The batch (mcd_batch_*, k = m = 16, 1 GB each) runs until every
-point's energy is at or below the reference's + 1e-6 Ha, retiring each point
-when it gets there.  Each point must get there, and not below the reference's
-own limit by more than its convergence still allows (the remaining decrease
+history.  On some points the reference stops early ("Factorization fails!",
+exit status 255, src/solver.h:444-450); there the energy to reach is its last
+reported one, and a point that failed before its first report has none.
+The batch (mcd_batch_*, k = m = 16, 1 GB each) runs until every point with an
+energy is at or below it + 1e-6 Ha, retiring each point when it gets there
+(the others at their first report).  Each such point must get there, and a
+point whose reference run completed must not go below the reference's own
+limit by more than its convergence still allows (the remaining decrease
 estimated from the reference's last reports, geometric tail, times three,
 plus 1e-6 Ha): the energy is variational, so a value far below the
 reference's would mean a different Hamiltonian.
@@ -54,12 +58,16 @@ def test_batched_curve_reaches_reference_energies(tmp_path):
         p = os.path.join(str(tmp_path), f"p{i:02d}.fcidump")
         synth.write_fcidump(p, "n16_5a5b", seed=0, t=i / 31)
         paths.append(p)
-    target = [ref[i]["energy"] + TOL for i in range(32)]
+    target = [None if ref[i]["energy"] is None else ref[i]["energy"] + TOL for i in range(32)]
+    want = sorted(i for i in range(32) if target[i] is not None)
+    assert len(want) >= 16, "fewer than half of the reference's runs left an energy"
     reached = {}
     b = m.CDFCIBatch([m.Fcidump(p) for p in paths], num_of_coordinate=16, estimate=16, max_memory=1.0,
                      z_threshold=0.0, threshold=0.0, num_iterations=400000, report_interval=500)
 
     def cb(i, r):
+        if target[i] is None:
+            return "retire"
         if r["energy"] <= target[i]:
             reached[i] = (r["iteration"], r["energy"])
             return "retire"
@@ -67,7 +75,9 @@ def test_batched_curve_reaches_reference_energies(tmp_path):
 
     b.solve(callback=cb)
     b.close()
-    assert sorted(reached) == list(range(32)), sorted(set(range(32)) - set(reached))
+    assert sorted(reached) == want, sorted(set(want) - set(reached))
     for i, (it, e) in reached.items():
-        low = ref[i]["energy"] - 3 * _tail(ref[i]["reports"]) - TOL
-        assert low <= e <= target[i], (i, it, e, ref[i]["energy"])
+        assert e <= target[i], (i, it, e, ref[i]["energy"])
+        if "failed" not in ref[i]:
+            low = ref[i]["energy"] - 3 * _tail(ref[i]["reports"]) - TOL
+            assert low <= e, (i, it, e, ref[i]["energy"])

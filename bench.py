@@ -527,10 +527,16 @@ def write_workload(d, seed):
 # ---------------------------------------------------------------------------
 # The reference solver, built from its sources (oracle/Makefile).
 
+REF_ATTEMPTS = 4
+
+
 def run_reference(fcidump, k, m, zt, warmup, steps, max_memory, threads):
     """Runs cdfci_omp for warmup+steps iterations; returns (updates/s, k_eff,
     seconds) measured from its own cumulative timer between the report at
-    `warmup` and the one at `warmup+steps`."""
+    `warmup` and the one at `warmup+steps`.  The reference's OpenMP runs do
+    not repeat one another, and some stop with "Factorization fails!" (exit
+    status 255, src/solver.h:444-450); such a run is started again, up to
+    REF_ATTEMPTS runs in all."""
     r = math.gcd(warmup, steps) if warmup > 0 else steps
     with tempfile.TemporaryDirectory() as d:
         deck = os.path.join(d, "input.json")
@@ -542,9 +548,12 @@ def run_reference(fcidump, k, m, zt, warmup, steps, max_memory, threads):
                                             "coordinate_update": "eig", "num_of_coordinate": k,
                                             "estimate": m}}}, f)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
-        res = subprocess.run([REF_EXE, deck], capture_output=True, text=True, env=env, timeout=1800)
+        for attempt in range(REF_ATTEMPTS):
+            res = subprocess.run([REF_EXE, deck], capture_output=True, text=True, env=env, timeout=1800)
+            if res.returncode == 0 or "Factorization fails" not in res.stdout:
+                break
     if res.returncode != 0:
-        raise RuntimeError("reference failed: " + (res.stderr or res.stdout)[-500:])
+        raise RuntimeError(f"reference failed ({attempt + 1} runs): " + (res.stderr or res.stdout)[-500:])
     k_eff = k
     m_warn = re.search(r"Not enough processes\. Set k = (\d+)", res.stdout)
     if m_warn:

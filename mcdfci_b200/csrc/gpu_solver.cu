@@ -358,7 +358,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   nb_ = __builtin_popcountll(ref_.b);
   if (na_ >= 64)  // its only determinant would carry the empty-slot key
     throw McdError(MCD_ERR_UNSUPPORTED, "64 alpha electrons in 64 orbitals (a single determinant) is not supported.");
-  entries_ = column_entries(ham_.norb, na_, nb_);
+  entries_ = column_entries(fci.norb / 2, na_, nb_);
   if (entries_ < 0) throw McdError(MCD_ERR_UNSUPPORTED, "a Hamiltonian column has more than 2^31 entries.");
   n_words_ = 1 + (fci.norb - 1) / 64;
 

@@ -434,7 +434,23 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     off = align_up(off + std::max<size_t>(n_vss, 1) * 8, 256);
     const size_t o_wab = off;
     off = align_up(off + n_wab * 8, 256);
-    d_tables_ = device_alloc<unsigned char>(off, "hamiltonian tables");
+    // The iteration's small buffers, in the same allocation after the tables.
+    // Per-CTA partial lists for the largest CTA count the autotuner tries.
+    const size_t parts = static_cast<size_t>(opt_.k) * std::max(groups_, opt_.autotune ? kMaxGroups : 1);
+    const size_t mk = static_cast<size_t>(kMaxK) * opt_.m;
+    size_t mo = off;
+    auto carve = [&](size_t bytes) {
+      const size_t o = mo;
+      mo = align_up(mo + bytes, 256);
+      return o;
+    };
+    const size_t o_state = carve(sizeof(IterState)), o_cs = carve(mk * sizeof(double)),
+                 o_cl = carve(mk * sizeof(unsigned)), o_h = carve(static_cast<size_t>(kMaxK) * kMaxK * sizeof(double)),
+                 o_err = carve(sizeof(unsigned)), o_occ = carve(sizeof(unsigned long long)),
+                 o_sect = carve((kLeaderSections + kColumnSections) * sizeof(unsigned long long)),
+                 o_pk = carve(parts * list_ * sizeof(unsigned long long)), o_ps = carve(parts * list_ * sizeof(unsigned)),
+                 o_psum = carve(parts * kPartSum * sizeof(double)), o_done = carve(kMaxK * sizeof(unsigned));
+    d_tables_ = device_alloc<unsigned char>(mo, "hamiltonian tables and iteration buffers");
     unsigned char* base = static_cast<unsigned char*>(d_tables_);
     auto up = [&](size_t o, const void* src, size_t bytes) {
       if (bytes) check(cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, stream_), "upload tables");
@@ -460,24 +476,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     } else {
       d_slots_ = device_alloc<Slot>(capacity_, "hash wavefunction");
     }
-    // The iteration's small buffers in one allocation.
-    // Per-CTA partial lists for the largest CTA count the autotuner tries.
-    const size_t parts = static_cast<size_t>(opt_.k) * std::max(groups_, opt_.autotune ? kMaxGroups : 1);
-    const size_t mk = static_cast<size_t>(kMaxK) * opt_.m;
-    size_t mo = 0;
-    auto carve = [&](size_t bytes) {
-      const size_t o = mo;
-      mo = align_up(mo + bytes, 256);
-      return o;
-    };
-    const size_t o_state = carve(sizeof(IterState)), o_cs = carve(mk * sizeof(double)),
-                 o_cl = carve(mk * sizeof(unsigned)), o_h = carve(static_cast<size_t>(kMaxK) * kMaxK * sizeof(double)),
-                 o_err = carve(sizeof(unsigned)), o_occ = carve(sizeof(unsigned long long)),
-                 o_sect = carve((kLeaderSections + kColumnSections) * sizeof(unsigned long long)),
-                 o_pk = carve(parts * list_ * sizeof(unsigned long long)), o_ps = carve(parts * list_ * sizeof(unsigned)),
-                 o_psum = carve(parts * kPartSum * sizeof(double)), o_done = carve(kMaxK * sizeof(unsigned));
-    d_misc_ = device_alloc<unsigned char>(mo, "iteration buffers");
-    unsigned char* mb = static_cast<unsigned char*>(d_misc_);
+    unsigned char* mb = static_cast<unsigned char*>(d_tables_);
     d_state_ = reinterpret_cast<IterState*>(mb + o_state);
     d_cand_score_ = reinterpret_cast<double*>(mb + o_cs);
     d_cand_slot_ = reinterpret_cast<unsigned*>(mb + o_cl);

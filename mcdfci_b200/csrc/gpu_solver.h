@@ -199,7 +199,7 @@ class GpuSolver {
   bool own_stream_ = false;
   int device_ = 0;
   void* d_tables_ = nullptr;
-  void* d_misc_ = nullptr;  // one allocation holding every buffer from d_state_ to d_done_
+  void* d_misc_ = nullptr;  // unused: the buffers from d_state_ to d_done_ follow the tables in d_tables_
   Slot* d_slots_ = nullptr;
   IterState* d_state_ = nullptr;
   double* d_cand_score_ = nullptr;

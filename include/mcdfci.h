@@ -374,6 +374,12 @@ int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_
  * *n_out receives the count.  No counterpart in the reference. */
 int mcd_debug_slots(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, double* z, int64_t cap,
                     int64_t* n_out);
+/* The inputs of the last iteration's subspace eigenproblem, the arguments of
+ * CoordinateUpdateEig::operator() (src/solver.h:333-345): H_sub (k x k,
+ * row-major), the picked coordinates' x and z before the update, and the
+ * double-double xx and xz.  *k_out = k; nothing is written when k > cap. */
+int mcd_debug_last_eig(mcd_solver* s, double* hsub, double* x, double* z, double xx[2], double xz[2], int32_t cap,
+                       int32_t* k_out);
 /* The determinants picked in the last iteration (alpha, beta, dx); *k_out <= cap. */
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out);
 

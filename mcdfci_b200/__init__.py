@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "mcd_create", "mcd_create_from_fcidump", "mcd_destroy", "mcd_solve", "mcd_reset",
     "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
-    "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_launch_info", "mcd_debug_leader_sections",
+    "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_last_eig", "mcd_debug_launch_info", "mcd_debug_leader_sections",
     "mcd_debug_scatter_rate",
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
@@ -162,6 +162,7 @@ def library() -> ctypes.CDLL:
     L.mcd_batch_result.argtypes = [vp, _dp]
     L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_debug_last_eig.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
     L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
     L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
@@ -573,6 +574,24 @@ class CDFCI:
         _check(library().mcd_debug_picked(self._h, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
                                           dx.ctypes.data_as(_dp), cap, ctypes.byref(k)))
         return a[: k.value], b[: k.value], dx[: k.value]
+
+    def last_eig_inputs(self) -> dict:
+        """The last iteration's subspace-eigenproblem inputs: H_sub, x, z,
+        xx and xz (double-double pairs), as mcd_debug_eig takes them."""
+        import numpy as np
+
+        cap = 128
+        h = np.zeros(cap * cap)
+        x = np.zeros(cap)
+        z = np.zeros(cap)
+        xx = np.zeros(2)
+        xz = np.zeros(2)
+        k = ctypes.c_int32()
+        _check(library().mcd_debug_last_eig(self._h, h.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
+                                            z.ctypes.data_as(_dp), xx.ctypes.data_as(_dp), xz.ctypes.data_as(_dp),
+                                            cap, ctypes.byref(k)))
+        n = k.value
+        return {"k": n, "hsub": h[: n * n].reshape(n, n), "x": x[:n], "z": z[:n], "xx": xx, "xz": xz}
 
 
 class CDFCIBatch:

@@ -771,6 +771,15 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
   });
 }
 
+int mcd_debug_last_eig(mcd_solver* s, double* hsub, double* x, double* z, double xx[2], double xz[2], int32_t cap,
+                       int32_t* k_out) {
+  return guarded([&] {
+    if (!s || !k_out) return fail(MCD_ERR_INVALID, "NULL argument.");
+    *k_out = static_cast<int32_t>(s->impl->last_eig_inputs(hsub, x, z, xx, xz, cap));
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_picked(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* dx, int32_t cap, int32_t* k_out) {
   return guarded([&] {
     if (!s || !k_out) return fail(MCD_ERR_INVALID, "NULL argument.");

@@ -445,7 +445,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
       return o;
     };
     const size_t o_state = carve(sizeof(IterState)), o_cs = carve(mk * sizeof(double)),
-                 o_cl = carve(mk * sizeof(unsigned)), o_h = carve(static_cast<size_t>(kMaxK) * kMaxK * sizeof(double)),
+                 o_cl = carve(mk * sizeof(unsigned)), o_h = carve((static_cast<size_t>(kMaxK) * kMaxK + 2 * kMaxK + 4) * sizeof(double)),
                  o_err = carve(sizeof(unsigned)), o_occ = carve(sizeof(unsigned long long)),
                  o_sect = carve((kLeaderSections + kColumnSections) * sizeof(unsigned long long)),
                  o_pk = carve(parts * list_ * sizeof(unsigned long long)), o_ps = carve(parts * list_ * sizeof(unsigned)),
@@ -1524,6 +1524,23 @@ std::vector<unsigned long long> GpuSolver::leader_sections() {
   check(cudaMemcpy(v.data(), d_sect_, v.size() * 8, cudaMemcpyDeviceToHost), "copy");
   check(cudaMemset(d_sect_, 0, v.size() * 8), "memset");
   return v;
+}
+
+int GpuSolver::last_eig_inputs(double* hsub, double* x, double* z, double xx[2], double xz[2], int cap) {
+  read_state();
+  const int k = h_state_.k_cur;
+  std::vector<double> buf(static_cast<size_t>(kMaxK) * kMaxK + 2 * kMaxK + 4);
+  check(cudaMemcpy(buf.data(), d_hsub_, buf.size() * sizeof(double), cudaMemcpyDeviceToHost), "read eig inputs");
+  if (k > cap) return k;
+  const double* in = buf.data() + static_cast<size_t>(kMaxK) * kMaxK;
+  for (int i = 0; i < k * k; ++i) if (hsub) hsub[i] = buf[i];
+  for (int i = 0; i < k; ++i) {
+    if (x) x[i] = in[i];
+    if (z) z[i] = in[kMaxK + i];
+  }
+  if (xx) { xx[0] = in[2 * kMaxK]; xx[1] = in[2 * kMaxK + 1]; }
+  if (xz) { xz[0] = in[2 * kMaxK + 2]; xz[1] = in[2 * kMaxK + 3]; }
+  return k;
 }
 
 std::vector<std::pair<Det, double>> GpuSolver::picked() {

@@ -94,6 +94,8 @@ class GpuSolver {
   // end of the last iteration.
   void slots(std::vector<Slot>& out);
   std::vector<std::pair<Det, double>> picked();
+  // The last eig update's inputs: k, H_sub (k x k), x, z (k each), xx, xz.
+  int last_eig_inputs(double* hsub, double* x, double* z, double xx[2], double xz[2], int cap);
   // Spin-summed spatial 1- and 2-RDM of the current wavefunction, normalised
   // (rdm1[P*n+Q] = sum_s <a+_{Ps} a_{Qs}>, rdm2[((P*n+Q)*n+R)*n+S] =
   // sum_{s,t} <a+_{Ps} a+_{Qt} a_{St} a_{Rs}>, n spatial orbitals), so that

@@ -99,7 +99,8 @@ struct LeaderLaunch {
   IterState* st;
   const double* cand_score;
   const unsigned* cand_slot;
-  double* hsub_out;       // [kMaxK*kMaxK] last H_sub (row-major, k_cur x k_cur)
+  double* hsub_out;       // [kMaxK*kMaxK] last H_sub (row-major, k_cur x k_cur), then the last eig
+                          // update's other inputs: x[kMaxK], z[kMaxK], xx (hi, lo), xz (hi, lo)
   unsigned long long* sect;  // [kLeaderSections] SM cycles per phase of the leader kernel, or null
   int m;
   int k_req;

@@ -848,6 +848,19 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   clk.mark(6);
   if (h_in_smem)
     for (int t = tid; t < k * k; t += kLT) L.hsub_out[t] = Hs[t];
+  {
+    double* in = L.hsub_out + kMaxK * kMaxK;
+    if (tid < k) {
+      in[tid] = s_x[tid];
+      in[kMaxK + tid] = s_z[tid];
+    }
+    if (tid == 0) {
+      in[2 * kMaxK] = sS.xx.hi;
+      in[2 * kMaxK + 1] = sS.xx.lo;
+      in[2 * kMaxK + 2] = sS.xz.hi;
+      in[2 * kMaxK + 3] = sS.xz.lo;
+    }
+  }
 
   // 6. Eig update.
   const EigResult er =

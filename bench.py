@@ -93,7 +93,7 @@ def parse_args():
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
     ap.add_argument("--phase-workload", default="n24_6a6b")
-    ap.add_argument("--eig-shift", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--eig-method", type=int, default=0, choices=[0, 1, 2],
                     help="subspace eigenproblem: 1 shifted inverse iteration first, 0 the full reduction")
     ap.add_argument("--scatter-sweep", action="store_true",
                     help="with --phases: also sweep the table's scattered-access probe")
@@ -401,7 +401,7 @@ def phases_arm(args, local_rank):
         synth.write_fcidump(path, args.phase_workload, seed=args.seed)
         s = mc.CDFCI(mc.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                      z_threshold=args.z_threshold, threshold=0.0, groups=args.groups, device=local_rank,
-                     eig_shift=args.eig_shift, num_iterations=args.warmup + args.steps)
+                     eig_method=args.eig_method, num_iterations=args.warmup + args.steps)
         s.reset()
         s.run_iterations(args.warmup)
         rb = s.report()
@@ -426,8 +426,8 @@ def phases_arm(args, local_rank):
                             scatter.append({"mode": name, "slots": entries, "ctas_per_sm": cps, "ilp": ilp,
                                             "slots_per_s": r, "us_per_launch": entries / r * 1e6})
         rep = s.report()
-        eig = {"shifted_updates": rep["inv_updates"] - rb["inv_updates"],
-               "shifted_steps_avg": (rep["inv_steps"] - rb["inv_steps"]) / max(1, rep["inv_updates"] - rb["inv_updates"]),
+        eig = {"fast_updates": rep["inv_updates"] - rb["inv_updates"],
+               "fast_steps_avg": (rep["inv_steps"] - rb["inv_steps"]) / max(1, rep["inv_updates"] - rb["inv_updates"]),
                "fallbacks": rep["eig_fallbacks"] - rb["eig_fallbacks"], "max_residual": rep["max_residual"]}
         groups = s.launch_info()["groups"]
         s.close()
@@ -440,7 +440,7 @@ def phases_arm(args, local_rank):
         "column_cycles_per_round": {k: round(v / rounds) for k, v in col.items()},
         "column_cycles_per_cta": per_cta,
         "column_rounds_per_cta": round(rounds / ctas, 2),
-        "energy": rep["energy"], "z_size": rep["z_size"], "eig": eig, "eig_shift": args.eig_shift,
+        "energy": rep["energy"], "z_size": rep["z_size"], "eig": eig, "eig_method": args.eig_method,
         "scatter_probe": scatter,
     }, indent=1))
     return 0

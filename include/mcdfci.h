@@ -104,9 +104,15 @@ typedef struct mcd_options {
    * explicit inverse, with the full reduction when that fails.  On 24
    * orbitals, k = 32, the shifted solver costs
    * as much as the reduction late in a solve and more early on (it needs
-   * more steps while the energy still drops fast), hence the default.  No
-   * counterpart in the reference (LAPACK dsyevr, src/solver.h:400-411). */
-  int32_t eig_shift;
+   * more steps while the energy still drops fast).  2: first by the bordered
+   * fixed point: with B = [[a, b'], [b, H_sub]], v = (1, y), one warp
+   * iterates y <- -(b + E y) / (d - lambda), lambda <- a + b'y (d the diagonal
+   * of H_sub, E the rest), and the result is taken when lambda plus the
+   * residual norm lies below the Gershgorin bound of H_sub, which makes it the
+   * lowest eigenvalue (Cauchy interlacing); the full reduction otherwise, or
+   * for k > 64.  No counterpart in the reference (LAPACK dsyevr,
+   * src/solver.h:400-411). */
+  int32_t eig_method;
   /* 1: with groups = 0, the CTAs per Hamiltonian column are chosen from
    * timed trials the first time at least 16 iterations per candidate are run
    * (the trials are iterations of the solve), among values around the fixed
@@ -292,6 +298,13 @@ int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* 
 int mcd_debug_eig_shifted(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                           const double xz[2], double drop, double* dx, double new_xx[2], double new_scale[2],
                           int32_t* branch, int32_t* steps);
+/* mcd_debug_eig with a given method, as mcd_options.eig_method selects it:
+ * 0 the full reduction, 1 shifted inverse iteration first (`drop` > 0 as in
+ * mcd_debug_eig_shifted), 2 the bordered fixed point first (`drop` unused).
+ * *steps receives the fast method's steps, 0 when the reduction ran. */
+int mcd_debug_eig_method(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                         const double xz[2], int32_t method, double drop, double* dx, double new_xx[2],
+                         double new_scale[2], int32_t* branch, int32_t* steps);
 /* mcd_debug_eig without any allocation: no counterpart in the reference.
  * The same kernel and results, but its device buffers are a file-scope
  * static device array of 134 KB (k <= 128; a larger k returns

@@ -46,7 +46,7 @@ EXPORTED_SYMBOLS = (
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
     "mcd_batch_run_iterations", "mcd_batch_run_iterations_timed", "mcd_batch_get_report", "mcd_batch_result",
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
-    "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted",
+    "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted", "mcd_debug_eig_method",
     "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual", "mcd_debug_scatter_rate_mode",
     "mcd_debug_autotune_info", "mcd_batch_table_sums",
 )
@@ -78,7 +78,7 @@ class mcd_options(ctypes.Structure):
         ("coordinate_pick", ctypes.c_int32), ("coordinate_update", ctypes.c_int32),
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
-        ("table_growth", ctypes.c_int32), ("eig_shift", ctypes.c_int32), ("autotune", ctypes.c_int32),
+        ("table_growth", ctypes.c_int32), ("eig_method", ctypes.c_int32), ("autotune", ctypes.c_int32),
     ]
 
 
@@ -144,6 +144,8 @@ def library() -> ctypes.CDLL:
                                         ctypes.POINTER(ctypes.c_int32), vp]
     L.mcd_debug_eig_shifted.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, ctypes.c_double, _dp, _dp, _dp,
                                         ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.mcd_debug_eig_method.argtypes = [ctypes.c_int32, _dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_double, _dp,
+                                       _dp, _dp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
     L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
     L.mcd_debug_column_sections.argtypes = [vp, _u64p, ctypes.c_int32, ctypes.c_int32]
@@ -296,7 +298,7 @@ def make_options(**kw) -> mcd_options:
     """mcd_options with the reference defaults, then keyword overrides
     (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
     z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
-    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth, eig_shift)."""
+    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth, eig_method)."""
     o = mcd_options()
     library().mcd_options_default(ctypes.byref(o))
     occ = kw.pop("ref_det_occ", None)
@@ -308,8 +310,8 @@ def make_options(**kw) -> mcd_options:
             o.stream = ctypes.c_void_p(int(v) if v else 0)
         elif k == "z_threshold_search":
             o.z_threshold_search = int(bool(v))
-        elif k == "eig_shift":
-            o.eig_shift = int(v)
+        elif k == "eig_method":
+            o.eig_method = int(v)
         elif k in ("compaction", "table_growth", "autotune"):
             setattr(o, k, int(bool(v)))
         else:
@@ -535,7 +537,7 @@ class CDFCI:
 
     LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
-                       "rayleigh", "eig_finish", "shifted", "shift_cholesky", "shift_inverse", "shift_power",
+                       "rayleigh", "eig_finish", "fast_solver", "shift_cholesky", "shift_inverse", "shift_power",
                        "shift_refine")
 
     def leader_sections(self) -> dict:
@@ -728,6 +730,25 @@ def debug_eig_shifted(hsub, x, z, xx, xz, drop):
     _check(library().mcd_debug_eig_shifted(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
                                            z.ctypes.data_as(_dp), xxa, xza, float(drop), dx.ctypes.data_as(_dp),
                                            nxx, nsc, ctypes.byref(br), ctypes.byref(st)))
+    return dx, tuple(nxx), tuple(nsc), br.value, st.value
+
+
+def debug_eig_method(hsub, x, z, xx, xz, method, drop=0.0):
+    """debug_eig with a given method (mcd_options.eig_method): 0 the full
+    reduction, 1 shifted inverse iteration first (drop > 0), 2 the bordered
+    fixed point first.  Returns (dx, new_xx, new_scale, branch, steps); steps
+    = 0 when the full reduction ran."""
+    import numpy as np
+
+    hsub, x, z, k = _eig_inputs(hsub, x, z)
+    dx = np.zeros(k)
+    nxx, nsc = (ctypes.c_double * 2)(), (ctypes.c_double * 2)()
+    br, st = ctypes.c_int32(), ctypes.c_int32()
+    xxa = (ctypes.c_double * 2)(*xx)
+    xza = (ctypes.c_double * 2)(*xz)
+    _check(library().mcd_debug_eig_method(k, hsub.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
+                                          z.ctypes.data_as(_dp), xxa, xza, int(method), float(drop),
+                                          dx.ctypes.data_as(_dp), nxx, nsc, ctypes.byref(br), ctypes.byref(st)))
     return dx, tuple(nxx), tuple(nsc), br.value, st.value
 
 

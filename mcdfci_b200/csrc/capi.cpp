@@ -72,8 +72,8 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   s.groups = o->groups;
   s.compaction = o->compaction != 0;
   s.table_growth = o->table_growth != 0;
-  if (o->eig_shift < 0 || o->eig_shift > 1) throw mcd::McdError(MCD_ERR_INVALID, "eig_shift must be 0 or 1.");
-  s.eig_shift = o->eig_shift;
+  if (o->eig_method < 0 || o->eig_method > 2) throw mcd::McdError(MCD_ERR_INVALID, "eig_method must be 0, 1 or 2.");
+  s.eig_method = o->eig_method;
   s.autotune = o->autotune != 0;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
@@ -159,7 +159,7 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   if (cd.has("groups")) o->groups = static_cast<int32_t>(cd.at("groups").as_number("groups"));
   if (cd.has("compaction")) o->compaction = cd.at("compaction").as_bool("compaction") ? 1 : 0;
   if (cd.has("table_growth")) o->table_growth = cd.at("table_growth").as_bool("table_growth") ? 1 : 0;
-  if (cd.has("eig_shift")) o->eig_shift = static_cast<int32_t>(cd.at("eig_shift").as_number("eig_shift"));
+  if (cd.has("eig_method")) o->eig_method = static_cast<int32_t>(cd.at("eig_method").as_number("eig_method"));
   if (cd.has("autotune")) o->autotune = cd.at("autotune").as_bool("autotune") ? 1 : 0;
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
@@ -197,7 +197,7 @@ void mcd_options_default(mcd_options* o) {
   o->groups = 0;
   o->compaction = 0;
   o->table_growth = 1;
-  o->eig_shift = 0;
+  o->eig_method = 0;
   o->autotune = 0;
   o->verbose = 0;
   o->stream = nullptr;
@@ -501,8 +501,8 @@ namespace {
 // mcd_debug_eig / mcd_debug_eig_shifted: one eig update on the current device
 // from host buffers; the device buffers are released on every path.
 int debug_eig_host(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
-                   const double xz[2], double drop, double* dx, double new_xx[2], double new_scale[2],
-                   int32_t* branch, int32_t* steps) {
+                   const double xz[2], double drop, int method, double* dx, double new_xx[2],
+                   double new_scale[2], int32_t* branch, int32_t* steps) {
   if (k < 1 || k > mcd::kMaxK) return fail(MCD_ERR_UNSUPPORTED, "k must be in 1..128.");
   if (!hsub || !x || !z || !xx || !xz || !dx || !new_xx || !new_scale) return fail(MCD_ERR_INVALID, "NULL argument.");
   struct Buffers {
@@ -537,7 +537,7 @@ int debug_eig_host(int32_t k, const double* hsub, const double* x, const double*
   ck(cudaMemcpy(b.z, z, sizeof(double) * k, cudaMemcpyHostToDevice));
   ck(cudaMemset(b.steps, 0, sizeof(int)));
   ck(mcd::debug_eig(k, b.h, b.x, b.z, mcd::dd{xx[0], xx[1]}, mcd::dd{xz[0], xz[1]}, b.dx, b.out, b.br, b.err, 0,
-                    drop, b.steps));
+                    drop, b.steps, method));
   mcd::dd out[2];
   int br = 0, st = 0;
   unsigned err = 0;
@@ -562,7 +562,7 @@ extern "C" {
 
 int mcd_debug_eig(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
                   const double xz[2], double* dx, double new_xx[2], double new_scale[2], int32_t* branch) {
-  return guarded([&] { return debug_eig_host(k, hsub, x, z, xx, xz, 0.0, dx, new_xx, new_scale, branch, nullptr); });
+  return guarded([&] { return debug_eig_host(k, hsub, x, z, xx, xz, 0.0, 0, dx, new_xx, new_scale, branch, nullptr); });
 }
 
 int mcd_debug_eig_shifted(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
@@ -570,7 +570,18 @@ int mcd_debug_eig_shifted(int32_t k, const double* hsub, const double* x, const 
                           int32_t* branch, int32_t* steps) {
   return guarded([&] {
     if (!(drop > 0.0)) return fail(MCD_ERR_INVALID, "drop must be positive.");
-    return debug_eig_host(k, hsub, x, z, xx, xz, drop, dx, new_xx, new_scale, branch, steps);
+    return debug_eig_host(k, hsub, x, z, xx, xz, drop, 1, dx, new_xx, new_scale, branch, steps);
+  });
+}
+
+int mcd_debug_eig_method(int32_t k, const double* hsub, const double* x, const double* z, const double xx[2],
+                         const double xz[2], int32_t method, double drop, double* dx, double new_xx[2],
+                         double new_scale[2], int32_t* branch, int32_t* steps) {
+  return guarded([&] {
+    if (method < 0 || method > 2) return fail(MCD_ERR_INVALID, "method must be 0, 1 or 2.");
+    if (method == 1 && !(drop > 0.0)) return fail(MCD_ERR_INVALID, "drop must be positive for method 1.");
+    return debug_eig_host(k, hsub, x, z, xx, xz, method == 1 ? drop : 0.0, method, dx, new_xx, new_scale, branch,
+                          steps);
   });
 }
 

@@ -1126,4 +1126,141 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
   return s_ok;
 }
 
+// ---------------------------------------------------------------------------
+// 6. The lowest eigenpair of the bordered matrix B = [[a, b'], [b, C]] (n = k + 1
+//    rows, k <= kBorderMaxK) when it lies below the Gershgorin bound of C,
+//    g = min_i (C_ii - sum_{j != i} |C_ij|).  By Cauchy interlacing B has exactly
+//    one eigenvalue below lambda_1(C) >= g, so an approximate eigenpair (lambda,
+//    v) with lambda + ||B v - lambda v|| / ||v|| < g belongs to the lowest
+//    eigenvalue (some eigenvalue lies within the residual norm of lambda).  With
+//    v = (1, y), D the diagonal of C and E the rest, the last k rows of
+//    (B - lambda I) v = 0 read (D - lambda I) y = -(b + E y), and the first row
+//    lambda = a + b'y.  One warp iterates
+//        y <- -(b + E y) / (d - lambda),   lambda <- a + b'y,
+//    which contracts by about max_i sum_j |E_ij| / (d_i - lambda) per step, less
+//    than 1 whenever lambda < g (C is strongly diagonal in a subspace of picked
+//    determinants, most of which are not connected by a single or double
+//    excitation).  The product E y of a step also gives the residual of the
+//    current iterate, r_i = (b + E y)_i + (d_i - lambda) y_i (row 0's residual
+//    is zero by the choice of lambda), so a step costs one matrix-vector
+//    product, one division per row and one warp reduction of three values, with
+//    no block barrier.  The iteration stops when ||r|| / ||v|| reaches
+//    1e-15 max_i sum_j |B_ij| (or stalls within 16 times that), and gives up
+//    when it stops contracting or lambda is not below g; A is only read.
+//    Returns true (uniform over the block) with V.y = (1, y) when the pair is
+//    certified; *iters receives the steps taken and *resid the final residual
+//    norm.  All threads call it.
+constexpr int kBorderMaxK = 64;
+constexpr int kBorderIters = 64;
+
+__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, int* iters, double* resid) {
+  __shared__ int s_ok, s_it;
+  __shared__ double s_rn;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int k = n - 1;
+  if (warp == 0) {
+    double* ys = V.y + 1;  // y_j at ys[j]
+    const double a = A[0];
+    double d[2], b[2], y[2];
+    bool own[2];
+    double gl = 1e300, nb = 0.0, babs = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int i = lane + 32 * q;
+      own[q] = i < k;
+      const double* row = A + (i + 1) * lda + 1;
+      d[q] = own[q] ? row[i] : 0.0;
+      b[q] = own[q] ? A[i + 1] : 0.0;
+      double off = 0.0;
+      if (own[q])
+        for (int j = 0; j < k; ++j) off += (j == i) ? 0.0 : fabs(row[j]);
+      y[q] = 0.0;
+      if (own[q]) {
+        gl = fmin(gl, d[q] - off);
+        nb = fmax(nb, fabs(d[q]) + off + fabs(b[q]));
+        babs += fabs(b[q]);
+        ys[i] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      gl = fmin(gl, __shfl_xor_sync(~0u, gl, o));
+      nb = fmax(nb, __shfl_xor_sync(~0u, nb, o));
+      babs += __shfl_xor_sync(~0u, babs, o);
+    }
+    nb = fmax(nb, fabs(a) + babs);
+    if (lane == 0) V.y[0] = 1.0;
+    __syncwarp();
+    const double tol = 1e-15 * nb;
+    double lam = fmin(a, gl) - 1e-3 * (1.0 + fabs(a));
+    double rprev = 1e300;
+    bool ok = false;
+    int t = 0;
+    for (; t < kBorderIters; ++t) {
+      // s = b + E y_t for this lane's rows.
+      double s[2], yn[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int i = lane + 32 * q;
+        const double* row = A + (i + 1) * lda + 1;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (own[q]) {
+          int j = 0;
+          for (; j + 3 < k; j += 4) {
+            s0 = fma(j == i ? 0.0 : row[j], ys[j], s0);
+            s1 = fma(j + 1 == i ? 0.0 : row[j + 1], ys[j + 1], s1);
+            s2 = fma(j + 2 == i ? 0.0 : row[j + 2], ys[j + 2], s2);
+            s3 = fma(j + 3 == i ? 0.0 : row[j + 3], ys[j + 3], s3);
+          }
+          for (; j < k; ++j) s0 = fma(j == i ? 0.0 : row[j], ys[j], s0);
+        }
+        s[q] = b[q] + ((s0 + s1) + (s2 + s3));
+        yn[q] = own[q] ? -s[q] / (d[q] - lam) : 0.0;
+      }
+      // Residual of (lambda_t, v_t), |y_t|^2 and b'y_{t+1}, in one reduction.
+      double rr = 0.0, yy = 0.0, by = 0.0;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (!own[q]) continue;
+        const double ri = fma(d[q] - lam, y[q], s[q]);
+        rr = fma(ri, ri, rr);
+        yy = fma(y[q], y[q], yy);
+        by = fma(b[q], yn[q], by);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        rr += __shfl_xor_sync(~0u, rr, o);
+        yy += __shfl_xor_sync(~0u, yy, o);
+        by += __shfl_xor_sync(~0u, by, o);
+      }
+      const double rn = sqrt(rr / (1.0 + yy));
+      if (!isfinite(rn)) break;
+      const bool small = rn <= tol || (t >= 2 && rn > 0.5 * rprev && rn <= 16.0 * tol);
+      if (t > 0 && small) {
+        ok = lam + rn < gl;
+        if (lane == 0) s_rn = rn;
+        break;
+      }
+      if ((t >= 8 && rn > 0.9 * rprev) || (t >= 4 && !(lam < gl))) break;
+      rprev = rn;
+      __syncwarp();  // every lane has read y_t
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        y[q] = yn[q];
+        if (own[q]) ys[lane + 32 * q] = yn[q];
+      }
+      lam = a + by;
+      __syncwarp();
+    }
+    if (lane == 0) {
+      s_ok = ok;
+      s_it = t + 1;
+    }
+  }
+  __syncthreads();
+  *iters = s_it;
+  if (resid) *resid = s_ok ? s_rn : 0.0;
+  return s_ok != 0;
+}
+
 }  // namespace mcd

@@ -544,7 +544,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.sect = d_sect_;
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
-  ll_.eig_shift = opt_.eig_shift;
+  ll_.eig_method = opt_.eig_method;
   check(cudaStreamSynchronize(stream_), "table upload");
   setup_ms_[1] = alloc_ms;
   setup_ms_[2] = ms_since(t_join);

@@ -104,7 +104,7 @@ struct LeaderLaunch {
   unsigned long long* sect;  // [kLeaderSections] SM cycles per phase of the leader kernel, or null
   int m;
   int k_req;
-  int eig_shift;          // 1: shifted inverse iteration first when the last energy drop is known
+  int eig_method;          // 1: shifted inverse iteration first when the last energy drop is known
 };
 
 // Several independent instances advanced by the same two launches per
@@ -218,7 +218,7 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
 // the reduction ran.
 cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
                       dd* xx_scale, int* branch, unsigned* err, cudaStream_t s, double drop = 0.0,
-                      int* steps = nullptr);
+                      int* steps = nullptr, int method = 1);
 size_t leader_smem_bytes(int k, int m);
 
 // debug_eig on HOST buffers with its device buffers in a file-scope device

@@ -181,7 +181,7 @@ __host__ __device__ constexpr size_t eig_work_doubles(int k) {
 // the reduction runs when that fails or its residual is not below 1e-11
 // (1 + |lambda|).
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
-                                double* dx, double* work, SectionClock& clk, double drop) {
+                                double* dx, double* work, SectionClock& clk, double drop, int method) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1, s_res;
   __shared__ int s_branch;
@@ -300,9 +300,19 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
       __syncthreads();
     }
   }
+  bool bordered = false;
+  if (!shifted && method == 2 && branch == 1 && k <= kBorderMaxK) {
+    int iters = 0;
+    double rn = 0.0;
+    bordered = eig_lowest_bordered(A, lda, n, V, &iters, &rn);
+    res.shift_steps = bordered ? iters : 0;
+    res.shift_diff = rn;
+    res.fallback = !bordered;
+  }
   clk.mark(16);
-  if (!shifted) eig_lowest(Ae, lda, n, V, clk);
+  if (!shifted && !bordered) eig_lowest(Ae, lda, n, V, clk);
   clk.mark(13);
+  shifted = shifted || bordered;  // a fast solve, checked below
 
   for (int attempt = 0; attempt < 2; ++attempt) {
   // B v in double, one row per warp (H is symmetric, so its rows are read).
@@ -864,7 +874,7 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
 
   // 6. Eig update.
   const EigResult er =
-      eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_shift ? sS.eig_drop : 0.0);
+      eig_update(Hs, k, s_x, s_z, sS.xx, sS.xz, s_dx, work, clk, L.eig_method == 1 ? sS.eig_drop : 0.0, L.eig_method);
   clk.mark(15);
   if (!er.ok) {
     if (tid == 0) {
@@ -999,7 +1009,7 @@ __device__ void symmetrise_from_upper(double* H, int k) {
 
 __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, const double* x, const double* z,
                                                            dd xx, dd xz, double* dx, dd* out, int* branch,
-                                                           unsigned* err, double drop, int* steps) {
+                                                           unsigned* err, double drop, int method, int* steps) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double s_x[kMaxK], s_z[kMaxK], s_dx[kMaxK];
   for (int i = threadIdx.x; i < k; i += blockDim.x) {
@@ -1008,7 +1018,8 @@ __global__ void __launch_bounds__(kLT, 1) debug_eig_kernel(int k, double* H, con
   }
   symmetrise_from_upper(H, k);
   SectionClock clk{nullptr, 0};
-  const EigResult er = eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, drop);
+  const EigResult er =
+      eig_update(H, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, drop, method);
   for (int i = threadIdx.x; i < k; i += blockDim.x) dx[i] = s_dx[i];
   if (threadIdx.x == 0) {
     out[0] = er.xx;
@@ -1095,12 +1106,13 @@ cudaError_t debug_hsub(const HamDev& h, const Det* dets, int k, double* hsub, cu
 }
 
 cudaError_t debug_eig(int k, double* hsub, const double* x, const double* z, dd xx, dd xz, double* dx,
-                      dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s, double drop, int* steps) {
+                      dd* new_xx_scale, int* branch, unsigned* err, cudaStream_t s, double drop, int* steps,
+                      int method) {
   const size_t bytes = eig_work_doubles(k) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(debug_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(bytes));
   if (e != cudaSuccess) return e;
-  debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err, drop, steps);
+  debug_eig_kernel<<<1, kLT, bytes, s>>>(k, hsub, x, z, xx, xz, dx, new_xx_scale, branch, err, drop, method, steps);
   return cudaGetLastError();
 }
 
@@ -1137,7 +1149,7 @@ __global__ void __launch_bounds__(kLT, 1) static_eig_kernel(int k, double* base,
   symmetrise_from_upper(base + kStaticEigH, k);
   SectionClock clk{nullptr, 0};
   const EigResult er =
-      eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, 0.0);
+      eig_update(base + kStaticEigH, k, s_x, s_z, xx, xz, s_dx, reinterpret_cast<double*>(smem), clk, 0.0, 0);
   for (int i = threadIdx.x; i < k; i += blockDim.x) base[kStaticEigDx + i] = s_dx[i];
   if (threadIdx.x == 0) {
     dd* out = reinterpret_cast<dd*>(base + kStaticEigOut);

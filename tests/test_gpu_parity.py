@@ -236,6 +236,67 @@ def test_eig_update_shifted_random_vs_numpy(k):
         assert abs(abs(_dd(nsc)) - abs(rsc)) < 1e-10 * abs(rsc)
 
 
+@pytest.mark.parametrize("fixture", ["eig_h2o.json.gz", "eig_n7.json.gz"])
+def test_eig_update_bordered_vs_reference_fixture(fixture):
+    """The bordered fixed point (eig_method 2) on the recorded reference calls:
+    same tolerances as the full reduction.  It certifies its eigenvalue as the
+    lowest when the eigenvalue plus the residual norm lies below the Gershgorin
+    bound of H_sub; the recorded calls but the first few certify, the others
+    take the reduction."""
+    g = load_golden(fixture)
+    taken = n = 0
+    for rec in g["calls"]:
+        if rec["call"] == 0:
+            continue
+        k = rec["k"]
+        H = np.array(rec["hsub"]).reshape(k, k)
+        dx, nxx, nsc, branch, steps = m.debug_eig_method(H, rec["x"], rec["z"], rec["xx"], rec["xz"], 2)
+        assert branch == 1
+        n += 1
+        taken += steps > 0
+        ref_dx = np.array(rec["dx"])
+        err = np.max(np.abs(dx - ref_dx) / (1.0 + np.abs(ref_dx)))
+        assert err < 1e-9, (rec["call"], steps, err)
+        assert abs(_dd(nxx) - _dd(rec["new_xx"])) <= 1e-12 * abs(_dd(rec["new_xx"])), (rec["call"], steps)
+        assert abs(abs(_dd(nsc)) - abs(_dd(rec["new_scale"]))) <= 1e-12 * abs(_dd(rec["new_scale"]))
+    assert taken >= n - 2, (taken, n)
+
+
+@pytest.mark.parametrize("k,coupling,certified", [(1, 0.02, True), (2, 0.02, True), (8, 0.02, True),
+                                                  (32, 0.02, True), (33, 0.02, True), (64, 0.01, True),
+                                                  (16, 1.5, False), (65, 0.01, False)])
+def test_eig_update_bordered_random_vs_numpy(k, coupling, certified):
+    """Bordered fixed point on random subproblems: B = [[a, b'], [b, C]] with C
+    diagonal plus symmetric couplings of the given size, (H, x, z, xx, xz)
+    derived so that the update rebuilds B.  Weak couplings keep lambda_1 below
+    C's Gershgorin bound (certified, steps > 0); strong ones do not, and k = 65
+    is beyond the method's 64 rows: the reduction runs (steps = 0).  Both
+    against numpy eigh."""
+    rng = np.random.default_rng(500 + k)
+    A = rng.normal(size=(k, k))
+    C = coupling * (A + A.T) / 2
+    np.fill_diagonal(C, -30.0 + rng.uniform(0, 5, k))
+    M = np.zeros((k + 1, k + 1))
+    M[0, 0] = -33.0
+    M[0, 1:] = M[1:, 0] = 0.3 * rng.normal(size=k)
+    M[1:, 1:] = C
+    w, U = np.linalg.eigh(M)
+    u = U[:, 0] * np.sign(U[0, 0])
+    y1 = 1.3 * u[0]
+    x = 1.3 * u[1:] + 1e-3 * rng.normal(size=k)
+    H = M[1:, 1:]
+    z = H @ x + y1 * M[0, 1:]
+    xx = float(y1 * y1 + x @ x)
+    xz = float(M[0, 0] * y1 * y1 + 2 * (x @ z) - x @ H @ x)
+    rdx, rxx, rsc = _eig_reference_numpy(H, x, z, xx, xz)
+    dx, nxx, nsc, branch, steps = m.debug_eig_method(H, x, z, (xx, 0.0), (xz, 0.0), 2)
+    assert branch == 1
+    assert (steps > 0) == certified, steps
+    assert np.max(np.abs(dx - rdx) / (1 + np.abs(rdx))) < 1e-9
+    assert abs(_dd(nxx) - rxx) < 1e-10 * abs(rxx)
+    assert abs(abs(_dd(nsc)) - abs(rsc)) < 1e-10 * abs(rsc)
+
+
 @pytest.mark.parametrize("k", [1, 4, 16])
 def test_eig_update_first_iteration_branch(k):
     rng = np.random.default_rng(100 + k)

@@ -21,6 +21,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <unistd.h>
 #include <cmath>
 #include <stdexcept>
 #include <thread>
@@ -30,23 +34,80 @@ namespace mcd {
 
 namespace {
 
-// f(i) for every i in [0, n) on up to 16 host threads, each taking the next
-// unclaimed i from a shared counter (the tasks differ in cost); every i
-// writes its own part of the tables, so no two threads share one.
-template <typename F>
-void parallel_tasks(int n, F f) {
-  const int hw = static_cast<int>(std::thread::hardware_concurrency());
-  const int nt = std::max(1, std::min({n, hw > 0 ? hw : 1, 16}));
-  std::atomic<int> next{0};
-  auto worker = [&] {
-    for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) f(i);
-  };
-  std::vector<std::thread> th;
-  th.reserve(nt - 1);
-  for (int t = 1; t < nt; ++t) th.emplace_back(worker);
-  worker();
-  for (auto& x : th) x.join();
-}
+// A pool of up to 15 worker threads, started on first use and kept for the
+// process: run(n, f) calls f(i) for every i in [0, n) on the workers and the
+// calling thread, each taking the next unclaimed i from a shared counter (the
+// tasks differ in cost), and returns when all are done.  Every i writes its
+// own part of the tables, so no two threads share one.  Calls from several
+// threads take turns.  A process forked from one that started the pool has
+// none of its threads, so it starts a pool of its own.
+class TaskPool {
+ public:
+  static TaskPool& get() {
+    static std::mutex mu;
+    static TaskPool* pool = nullptr;  // kept to the end of the process, like its threads
+    static pid_t owner = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pool || owner != getpid()) {
+      pool = new TaskPool();
+      owner = getpid();
+    }
+    return *pool;
+  }
+  void run(int n, const std::function<void(int)>& f) {
+    std::lock_guard<std::mutex> turn(run_mu_);
+    if (workers_ == 0 || n <= 1) {
+      for (int i = 0; i < n; ++i) f(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &f;
+      n_ = n;
+      next_.store(0);
+      busy_ = workers_;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work(f, n);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return busy_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  TaskPool() {
+    const int hw = static_cast<int>(std::thread::hardware_concurrency());
+    workers_ = std::max(0, std::min(hw > 0 ? hw : 1, 16) - 1);
+    for (int t = 0; t < workers_; ++t) std::thread([this] { loop(); }).detach();
+  }
+  void work(const std::function<void(int)>& f, int n) {
+    for (int i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) f(i);
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      const std::function<void(int)>* f;
+      int n;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        f = job_;
+        n = n_;
+      }
+      work(*f, n);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--busy_ == 0) done_cv_.notify_one();
+    }
+  }
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)>* job_ = nullptr;
+  int n_ = 0, busy_ = 0, workers_ = 0;
+  unsigned long long gen_ = 0;
+  std::atomic<int> next_{0};
+};
 
 }  // namespace
 
@@ -86,13 +147,15 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
     for (int j = i + 1; j < nso; ++j) h.d2[i * nso + j] = fci.g(i, j, i, j) - fci.g(i, j, j, i);
 
   // Singles, same-spin and opposite-spin doubles: one pool of tasks, the
-  // most expensive (opposite-spin rows) first.
+  // most expensive (opposite-spin rows) first.  Every task writes each entry
+  // of its rows (0 where the value is not above the threshold), so the
+  // tables need no clearing first.
   const size_t np = static_cast<size_t>(h.npair);
-  h.sh.assign(2 * static_cast<size_t>(n) * n, 0.0);
-  h.st.assign(2 * static_cast<size_t>(n) * n * nso, 0.0);
+  h.sh.resize(2 * static_cast<size_t>(n) * n);
+  h.st.resize(2 * static_cast<size_t>(n) * n * nso);
   h.spres.assign(2 * static_cast<size_t>(n), 0);
-  h.vss.assign(2 * np * np, 0.0);
-  h.wab.assign(static_cast<size_t>(n) * n * n * n, 0.0);
+  h.vss.resize(2 * np * np);
+  h.wab.resize(static_cast<size_t>(n) * n * n * n);
   // Single excitations p -> r of spin s, every r.
   auto singles = [&](int s, int p) {
     uint64_t pres = 0;
@@ -115,20 +178,22 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
     }
     h.spres[s * n + p] = pres;
   };
-  // Same-spin doubles out of the pairs (p, q), p < q, of spin s.
+  // Same-spin doubles out of the pairs (p, q), p < q, of spin s: rows P(p, q).
   auto same_spin = [&](int s, int q) {
     for (int p = 0; p < q; ++p) {
       const int i = 2 * p + s, j = 2 * q + s;
+      double* row = &h.vss[(s * np + pair_index(p, q)) * np];
       for (int ss = 1; ss < n; ++ss)
         for (int r = 0; r < ss; ++r) {
           const int a = 2 * r + s, b = 2 * ss + s;
           const double v = fci.g(i, j, a, b) - fci.g(i, j, b, a);
-          if (std::fabs(v) > thr) h.vss[(s * np + pair_index(p, q)) * np + pair_index(r, ss)] = v;
+          row[pair_index(r, ss)] = std::fabs(v) > thr ? v : 0.0;
         }
     }
   };
-  // Opposite-spin doubles out of alpha pa and beta pb.
+  // Opposite-spin doubles out of alpha pa and beta pb: n x n entries.
   auto opposite_spin = [&](int pa, int pb) {
+    double* blk = &h.wab[(static_cast<size_t>(pa) * n + pb) * n * n];
     for (int ra = 0; ra < n; ++ra)
       for (int sb = 0; sb < n; ++sb) {
         double v;
@@ -136,11 +201,11 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
           v = fci.g(2 * pa, 2 * pb + 1, 2 * ra, 2 * sb + 1);
         else
           v = fci.g(2 * pb + 1, 2 * pa, 2 * sb + 1, 2 * ra);
-        if (std::fabs(v) > thr) h.wab[((static_cast<size_t>(pa) * n + pb) * n + ra) * n + sb] = v;
+        blk[ra * n + sb] = std::fabs(v) > thr ? v : 0.0;
       }
   };
   const int n_ab = n * n, n_ss = 2 * n, n_s = 2 * n;
-  parallel_tasks(n_ab + n_ss + n_s, [&](int t) {
+  TaskPool::get().run(n_ab + n_ss + n_s, [&](int t) {
     if (t < n_ab) {
       opposite_spin(t / n, t % n);
     } else if (t < n_ab + n_ss) {

@@ -3,12 +3,36 @@
 #pragma once
 
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "fcidump.h"
 #include "mcd_types.h"
 
 namespace mcd {
+
+// std::allocator whose value construction leaves doubles uninitialised, for
+// tables that their builder writes in full.
+template <typename T>
+struct DefaultInitAllocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = DefaultInitAllocator<U>;
+  };
+  DefaultInitAllocator() = default;
+  template <typename U>
+  DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+using TableVec = std::vector<double, DefaultInitAllocator<double>>;
 
 struct HamHost {
   int norb = 0;   // spatial orbitals
@@ -17,11 +41,11 @@ struct HamHost {
   double ecore = 0.0;
   std::vector<double> hdiag;    // [nso]
   std::vector<double> d2;       // [nso*nso]
-  std::vector<double> sh;       // [2][norb][norb]
-  std::vector<double> st;       // [2][norb][norb][nso]
+  TableVec sh;                  // [2][norb][norb]
+  TableVec st;                  // [2][norb][norb][nso]
   std::vector<uint64_t> spres;  // [2][norb]
-  std::vector<double> vss;      // [2][npair][npair]
-  std::vector<double> wab;      // [norb^4]
+  TableVec vss;                 // [2][npair][npair]
+  TableVec wab;                 // [norb^4]
 };
 
 // Builds the tables.  `threshold` is hamiltonian:threshold: a double

@@ -93,7 +93,7 @@ def parse_args():
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
     ap.add_argument("--phase-workload", default="n24_6a6b")
-    ap.add_argument("--eig-method", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--eig-method", type=int, default=2, choices=[0, 1, 2],
                     help="subspace eigenproblem: 1 shifted inverse iteration first, 0 the full reduction")
     ap.add_argument("--scatter-sweep", action="store_true",
                     help="with --phases: also sweep the table's scattered-access probe")

@@ -96,21 +96,21 @@ typedef struct mcd_options {
    * reserves its table.  A growth that finds the device memory taken by
    * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
   int32_t table_growth;
-  /* 0 (default): every subspace eigenproblem by the full reduction
-   * (Householder, multisection, inverse iteration).  1: first by shifted
-   * inverse iteration (a Cholesky factorisation of B - sigma I, sigma below
-   * the current energy by 16 times the last energy drop, certifies sigma <
-   * lambda_1; the current vector starts it), its steps run by one warp on the
-   * explicit inverse, with the full reduction when that fails.  On 24
-   * orbitals, k = 32, the shifted solver costs
-   * as much as the reduction late in a solve and more early on (it needs
-   * more steps while the energy still drops fast).  2: first by the bordered
-   * fixed point: with B = [[a, b'], [b, H_sub]], v = (1, y), one warp
-   * iterates y <- -(b + E y) / (d - lambda), lambda <- a + b'y (d the diagonal
-   * of H_sub, E the rest), and the result is taken when lambda plus the
-   * residual norm lies below the Gershgorin bound of H_sub, which makes it the
-   * lowest eigenvalue (Cauchy interlacing); the full reduction otherwise, or
-   * for k > 64.  No counterpart in the reference (LAPACK dsyevr,
+  /* The subspace eigenproblem's method.  0: the full reduction for every
+   * update (Householder, multisection, inverse iteration).  1: first by
+   * shifted inverse iteration (a Cholesky factorisation of B - sigma I, sigma
+   * below the current energy by 16 times the last energy drop, certifies
+   * sigma < lambda_1; the current vector starts it), its steps run by one warp
+   * on the explicit inverse, with the full reduction when that fails.  2
+   * (default): first by the bordered fixed point: with B = [[a, b'], [b,
+   * H_sub]] and v = (1, y), one warp iterates y <- -(b + E y) / (d - lambda),
+   * lambda <- a + b'y (d the diagonal of H_sub, E the rest, kept as its
+   * nonzeros), and the result is taken when lambda plus the residual norm
+   * lies below the Gershgorin bound of H_sub, which makes it the lowest
+   * eigenvalue (Cauchy interlacing); the full reduction otherwise, and for
+   * k > 64.  On 24 orbitals, k = 32, method 2 certifies every update after the
+   * first few in 12-17 steps, method 1 costs as much as the reduction late in a
+   * solve and more early on.  No counterpart in the reference (LAPACK dsyevr,
    * src/solver.h:400-411). */
   int32_t eig_method;
   /* 1: with groups = 0, the CTAs per Hamiltonian column are chosen from

@@ -197,7 +197,7 @@ void mcd_options_default(mcd_options* o) {
   o->groups = 0;
   o->compaction = 0;
   o->table_growth = 1;
-  o->eig_method = 0;
+  o->eig_method = 2;
   o->autotune = 0;
   o->verbose = 0;
   o->stream = nullptr;

@@ -1144,7 +1144,12 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
 //    current iterate, r_i = (b + E y)_i + (d_i - lambda) y_i (row 0's residual
 //    is zero by the choice of lambda), so a step costs one matrix-vector
 //    product, one division per row and one warp reduction of three values, with
-//    no block barrier.  The iteration stops when ||r|| / ||v|| reaches
+//    no block barrier.  E is sparse (most picked determinants are not
+//    connected), so each lane first packs its rows' nonzero entries of E into
+//    `pack`, 2 (k + 1) lda doubles of scratch (values of row i from i lda on;
+//    after the k rows of values, their columns as 4-byte ints, row i from
+//    i (2 lda + 1) on), and a step's product runs over those only.  The
+//    iteration stops when ||r|| / ||v|| reaches
 //    1e-15 max_i sum_j |B_ij| (or stalls within 16 times that), and gives up
 //    when it stops contracting or lambda is not below g; A is only read.
 //    Returns true (uniform over the block) with V.y = (1, y) when the pair is
@@ -1153,7 +1158,8 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
 constexpr int kBorderMaxK = 64;
 constexpr int kBorderIters = 64;
 
-__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, int* iters, double* resid) {
+__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, double* pack, int* iters,
+                                    double* resid) {
   __shared__ int s_ok, s_it;
   __shared__ double s_rn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1163,7 +1169,12 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
     const double a = A[0];
     double d[2], b[2], y[2];
     bool own[2];
+    int cnt[2];
     double gl = 1e300, nb = 0.0, babs = 0.0;
+    // Row i's nonzero off-diagonal entries of C: values at pv + i lda, their
+    // columns at pc + i (2 lda + 1) (an odd stride in 4-byte words).
+    double* const pv = pack;
+    int* const pc = reinterpret_cast<int*>(pack + static_cast<size_t>(k) * lda);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int i = lane + 32 * q;
@@ -1172,8 +1183,18 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
       d[q] = own[q] ? row[i] : 0.0;
       b[q] = own[q] ? A[i + 1] : 0.0;
       double off = 0.0;
+      int c = 0;
       if (own[q])
-        for (int j = 0; j < k; ++j) off += (j == i) ? 0.0 : fabs(row[j]);
+        for (int j = 0; j < k; ++j) {
+          const double v = row[j];
+          if (j != i && v != 0.0) {
+            off += fabs(v);
+            pv[i * lda + c] = v;
+            pc[i * (2 * lda + 1) + c] = j;
+            ++c;
+          }
+        }
+      cnt[q] = c;
       y[q] = 0.0;
       if (own[q]) {
         gl = fmin(gl, d[q] - off);
@@ -1182,11 +1203,13 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
         ys[i] = 0.0;
       }
     }
+    int cmax = max(cnt[0], cnt[1]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       gl = fmin(gl, __shfl_xor_sync(~0u, gl, o));
       nb = fmax(nb, __shfl_xor_sync(~0u, nb, o));
       babs += __shfl_xor_sync(~0u, babs, o);
+      cmax = max(cmax, __shfl_xor_sync(~0u, cmax, o));
     }
     nb = fmax(nb, fabs(a) + babs);
     if (lane == 0) V.y[0] = 1.0;
@@ -1197,24 +1220,23 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
     bool ok = false;
     int t = 0;
     for (; t < kBorderIters; ++t) {
-      // s = b + E y_t for this lane's rows.
+      // s = b + E y_t for this lane's rows, over their packed nonzeros.
       double s[2], yn[2];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int i = lane + 32 * q;
-        const double* row = A + (i + 1) * lda + 1;
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        if (own[q]) {
-          int j = 0;
-          for (; j + 3 < k; j += 4) {
-            s0 = fma(j == i ? 0.0 : row[j], ys[j], s0);
-            s1 = fma(j + 1 == i ? 0.0 : row[j + 1], ys[j + 1], s1);
-            s2 = fma(j + 2 == i ? 0.0 : row[j + 2], ys[j + 2], s2);
-            s3 = fma(j + 3 == i ? 0.0 : row[j + 3], ys[j + 3], s3);
+        const double* rv = pv + i * lda;
+        const int* rc = pc + i * (2 * lda + 1);
+        double s0 = 0.0, s1 = 0.0;
+        if (q == 0 || k > 32) {
+          int e = 0;
+          for (; e + 1 < cmax; e += 2) {
+            if (e < cnt[q]) s0 = fma(rv[e], ys[rc[e]], s0);
+            if (e + 1 < cnt[q]) s1 = fma(rv[e + 1], ys[rc[e + 1]], s1);
           }
-          for (; j < k; ++j) s0 = fma(j == i ? 0.0 : row[j], ys[j], s0);
+          if (e < cmax && e < cnt[q]) s0 = fma(rv[e], ys[rc[e]], s0);
         }
-        s[q] = b[q] + ((s0 + s1) + (s2 + s3));
+        s[q] = b[q] + (s0 + s1);
         yn[q] = own[q] ? -s[q] / (d[q] - lam) : 0.0;
       }
       // Residual of (lambda_t, v_t), |y_t|^2 and b'y_{t+1}, in one reduction.

@@ -36,7 +36,7 @@ struct SolverOptions {
   bool table_growth = true;
   // Subspace eigenproblem: 0 the full reduction every time; 1 shifted
   // inverse iteration first, with the reduction when it fails.
-  int eig_method = 0;
+  int eig_method = 2;
   // Choose the CTAs per Hamiltonian column from timed trials (real
   // iterations of the solve) the first time enough iterations are run, and
   // remember the choice per (orbitals, electrons, k, m, SM count).

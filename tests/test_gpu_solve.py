@@ -28,9 +28,15 @@ def _solve(path, **kw):
     return s, e
 
 
-def test_h2o_matches_reference(fcidumps):
+@pytest.mark.parametrize("eig_method", [2, 0])
+def test_h2o_matches_reference(fcidumps, eig_method):
+    """Both the default subspace solver (the bordered fixed point) and the
+    full reduction reach the reference's energy."""
     s, e = _solve(fcidumps["h2o_sto3g"], num_iterations=20000, report_interval=1000, max_memory=0.005,
-                  num_of_coordinate=8, estimate=8)
+                  num_of_coordinate=8, estimate=8, eig_method=eig_method)
+    if eig_method == 2:
+        rep = s.report()
+        assert rep["inv_updates"] > 0.8 * 20000, rep["inv_updates"]  # the fixed point took nearly every update
     assert abs(e - ENERGIES["h2o_sto3g k8 m8 20000it"]) < 1e-6
     assert len(s.reports) == 20
     assert [r["iteration"] for r in s.reports] == [1000 * (i + 1) for i in range(20)]

@@ -537,8 +537,7 @@ class CDFCI:
 
     LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
-                       "rayleigh", "eig_finish", "fast_solver", "shift_cholesky", "shift_inverse", "shift_power",
-                       "shift_refine")
+                       "rayleigh", "eig_finish", "fast_solver", "fast_1", "fast_2", "fast_3", "fast_4")
 
     def leader_sections(self) -> dict:
         """SM cycles per leader-kernel phase since the previous call."""

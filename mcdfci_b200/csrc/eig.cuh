@@ -1159,7 +1159,7 @@ constexpr int kBorderMaxK = 64;
 constexpr int kBorderIters = 64;
 
 __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, double* pack, int* iters,
-                                    double* resid) {
+                                    double* resid, SectionClock& clk) {
   __shared__ int s_ok, s_it;
   __shared__ double s_rn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1214,9 +1214,13 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
     nb = fmax(nb, fabs(a) + babs);
     if (lane == 0) V.y[0] = 1.0;
     __syncwarp();
+    clk.mark(17);
     const double tol = 1e-15 * nb;
+    const double tol2 = tol * tol;
     double lam = fmin(a, gl) - 1e-3 * (1.0 + fabs(a));
-    double rprev = 1e300;
+    // The tests compare squared residual norms |r|^2 / |v|^2 cross-multiplied,
+    // so that no division or square root sits on a step's chain.
+    double rrp = 1e300, vvp = 1.0;  // |r|^2 and |v|^2 of the previous step
     bool ok = false;
     int t = 0;
     for (; t < kBorderIters; ++t) {
@@ -1227,18 +1231,26 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
         const int i = lane + 32 * q;
         const double* rv = pv + i * lda;
         const int* rc = pc + i * (2 * lda + 1);
-        double s0 = 0.0, s1 = 0.0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         if (q == 0 || k > 32) {
+          const int c = cnt[q];
           int e = 0;
-          for (; e + 1 < cmax; e += 2) {
-            if (e < cnt[q]) s0 = fma(rv[e], ys[rc[e]], s0);
-            if (e + 1 < cnt[q]) s1 = fma(rv[e + 1], ys[rc[e + 1]], s1);
+          for (; e + 3 < cmax; e += 4) {
+            if (e < c) s0 = fma(rv[e], ys[rc[e]], s0);
+            if (e + 1 < c) s1 = fma(rv[e + 1], ys[rc[e + 1]], s1);
+            if (e + 2 < c) s2 = fma(rv[e + 2], ys[rc[e + 2]], s2);
+            if (e + 3 < c) s3 = fma(rv[e + 3], ys[rc[e + 3]], s3);
           }
-          if (e < cmax && e < cnt[q]) s0 = fma(rv[e], ys[rc[e]], s0);
+          for (; e < cmax; ++e)
+            if (e < c) s0 = fma(rv[e], ys[rc[e]], s0);
+          s[q] = b[q] + ((s0 + s1) + (s2 + s3));
+          yn[q] = own[q] ? -s[q] / (d[q] - lam) : 0.0;
+        } else {
+          s[q] = 0.0;
+          yn[q] = 0.0;
         }
-        s[q] = b[q] + (s0 + s1);
-        yn[q] = own[q] ? -s[q] / (d[q] - lam) : 0.0;
       }
+      clk.mark(18);
       // Residual of (lambda_t, v_t), |y_t|^2 and b'y_{t+1}, in one reduction.
       double rr = 0.0, yy = 0.0, by = 0.0;
 #pragma unroll
@@ -1255,16 +1267,22 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
         yy += __shfl_xor_sync(~0u, yy, o);
         by += __shfl_xor_sync(~0u, by, o);
       }
-      const double rn = sqrt(rr / (1.0 + yy));
-      if (!isfinite(rn)) break;
-      const bool small = rn <= tol || (t >= 2 && rn > 0.5 * rprev && rn <= 16.0 * tol);
+      const double vv = 1.0 + yy;
+      if (!isfinite(rr) || !isfinite(vv)) break;
+      // rn <= tol, or rn > rn_prev / 2 and rn <= 16 tol (stalled at rounding)
+      const bool small =
+          rr <= tol2 * vv || (t >= 2 && rr * vvp > 0.25 * rrp * vv && rr <= 256.0 * tol2 * vv);
       if (t > 0 && small) {
+        const double rn = sqrt(rr / vv);
         ok = lam + rn < gl;
         if (lane == 0) s_rn = rn;
         break;
       }
-      if ((t >= 8 && rn > 0.9 * rprev) || (t >= 4 && !(lam < gl))) break;
-      rprev = rn;
+      // not contracting (rn > 0.9 rn_prev), or lambda not below g
+      if ((t >= 8 && rr * vvp > 0.81 * rrp * vv) || (t >= 4 && !(lam < gl))) break;
+      clk.mark(19);
+      rrp = rr;
+      vvp = vv;
       __syncwarp();  // every lane has read y_t
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
@@ -1273,6 +1291,7 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
       }
       lam = a + by;
       __syncwarp();
+      clk.mark(20);
     }
     if (lane == 0) {
       s_ok = ok;

@@ -149,9 +149,12 @@ struct RdmLaunch {
 // 7 update_x, 8 publish, 9 eig setup, 10 tridiagonalisation, 11 multisection,
 // 12 inverse iteration, 13 back-transformation, 14 Rayleigh quotient,
 // 15 eig finish,
-// 16 shifted inverse iteration (when it runs, in place of 10-13: its set-up
-// and, when it fails, the restore), split into 17 Cholesky factorisation,
-// 18 explicit inverse, 19 power steps, 20 refinement steps.
+// 16 the fast solver of eig_method 1 or 2 (when it runs, in place of 10-13:
+// its set-up and, when it fails, the restore), the rest of it in 17-20:
+// method 1: 17 Cholesky factorisation, 18 explicit inverse, 19 power steps,
+// 20 refinement steps; method 2: 17 packing of H_sub's nonzeros and the
+// bounds, 18 products and divisions of its steps, 19 their reductions and
+// tests, 20 their stores.
 constexpr int kLeaderSections = 21;
 
 // Phases of the column kernel timed into ColumnLaunch::sect (thread 0 of each

@@ -304,7 +304,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   if (!shifted && method == 2 && branch == 1 && k <= kBorderMaxK) {
     int iters = 0;
     double rn = 0.0;
-    bordered = eig_lowest_bordered(A, lda, n, V, Li, &iters, &rn, clk);  // Li and Ci as its scratch
+    bordered = eig_lowest_bordered(A, lda, n, V, &iters, &rn, clk);
     res.shift_steps = bordered ? iters : 0;
     res.shift_diff = rn;
     res.fallback = !bordered;

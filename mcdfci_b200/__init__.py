@@ -537,7 +537,8 @@ class CDFCI:
 
     LEADER_SECTIONS = ("state", "finish", "gather", "topk", "tie_sort", "picked", "hsub", "update_x",
                        "publish", "eig_setup", "tridiag", "multisection", "inv_iter", "backtransform",
-                       "rayleigh", "eig_finish", "fast_solver", "fast_1", "fast_2", "fast_3", "fast_4")
+                       "rayleigh", "eig_finish", "fast_solver", "fast_1", "fast_2", "fast_3", "fast_4",
+                       "setup_fill", "setup_hx", "setup_sums", "rq_product")
 
     def leader_sections(self) -> dict:
         """SM cycles per leader-kernel phase since the previous call."""

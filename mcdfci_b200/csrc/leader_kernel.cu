@@ -230,6 +230,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   };
   fill_h();
   __syncthreads();
+  clk.mark(21);
   // H x in double (dsymv, src/solver.h:355); x'x, x'z, x'Hx in double-double,
   // rounded where the reference works in double.
   for (int r = warp; r < k; r += kLW) {
@@ -240,6 +241,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     if (lane == 0) Hx[r] = s;
   }
   __syncthreads();
+  clk.mark(22);
   if (warp == 0) {
     dd sxx{0, 0}, sxz{0, 0}, sxhx{0, 0};
     for (int i = lane; i < k; i += 32) {
@@ -263,6 +265,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     }
   }
   __syncthreads();
+  clk.mark(23);
   const int branch = s_branch;
   const int n = branch == 1 ? k + 1 : k;
   const double y1 = s_y1;
@@ -333,6 +336,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
     if (lane == 0) Bv[r] = s;
   }
   __syncthreads();
+  clk.mark(24);
   // Rayleigh quotient y'By / y'y, normalisation in double-double, sign fix,
   // residual ||B v - lambda v||.
   if (warp == 0) {

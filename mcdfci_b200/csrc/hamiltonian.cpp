@@ -220,6 +220,8 @@ HamHost build_hamiltonian(const Fcidump& fci, double thr) {
   return h;
 }
 
+void host_parallel(int n, const std::function<void(int)>& f) { TaskPool::get().run(n, f); }
+
 Det det_from_spin_orbitals(const std::vector<int>& occ) {
   Det d{0, 0};
   for (int so : occ) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <string>
+#include <functional>
 #include <memory>
 #include <utility>
 #include <vector>
@@ -56,6 +57,10 @@ struct HamHost {
 // beta spin-orbitals (spin-changing excitations), none of which the
 // alpha/beta determinant layout represents.
 HamHost build_hamiltonian(const Fcidump& fci, double threshold);
+
+// f(i) for every i in [0, n) on the host task pool that builds the tables
+// (up to 16 threads, the caller included); returns when all are done.
+void host_parallel(int n, const std::function<void(int)>& f);
 
 // Determinant helpers (host).
 Det det_from_spin_orbitals(const std::vector<int>& occ);

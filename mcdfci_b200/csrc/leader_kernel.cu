@@ -184,6 +184,8 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
                                 double* dx, double* work, SectionClock& clk, double drop, int method) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_b00, s_y1, s_res;
+  __shared__ dd s_sum3[3];
+  __shared__ double s_sgn;
   __shared__ int s_branch;
   __shared__ dd s_rq;
   EigResult res;
@@ -242,18 +244,18 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   }
   __syncthreads();
   clk.mark(22);
+  // The three sums on warps 0, 1, 2 (each in the same order as alone).
+  if (warp < 3) {
+    const double* w = warp == 0 ? x : (warp == 1 ? z : Hx);
+    dd acc{0, 0};
+    for (int i = lane; i < k; i += 32) acc = dd_add(acc, dd_two_prod(x[i], w[i]));
+    acc = warp_sum_dd(acc);
+    if (lane == 0) s_sum3[warp] = acc;
+  }
+  __syncthreads();
   if (warp == 0) {
-    dd sxx{0, 0}, sxz{0, 0}, sxhx{0, 0};
-    for (int i = lane; i < k; i += 32) {
-      sxx = dd_add(sxx, dd_two_prod(x[i], x[i]));
-      sxz = dd_add(sxz, dd_two_prod(x[i], z[i]));
-      sxhx = dd_add(sxhx, dd_two_prod(x[i], Hx[i]));
-    }
-    sxx = warp_sum_dd(sxx);
-    sxz = warp_sum_dd(sxz);
-    sxhx = warp_sum_dd(sxhx);
     if (lane == 0) {
-      const double xTx = dd_to_d(sxx), xTz = dd_to_d(sxz), xTHx = dd_to_d(sxhx);
+      const double xTx = dd_to_d(s_sum3[0]), xTz = dd_to_d(s_sum3[1]), xTHx = dd_to_d(s_sum3[2]);
       const double yy = dd_to_d(dd_add_d(xx, -xTx));
       s_branch = fabs(yy) > 1e-14 ? 1 : 2;
       if (s_branch == 1) {
@@ -338,27 +340,42 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   __syncthreads();
   clk.mark(24);
   // Rayleigh quotient y'By / y'y, normalisation in double-double, sign fix,
-  // residual ||B v - lambda v||.
-  if (warp == 0) {
-    dd nrm{0, 0}, num{0, 0};
+  // residual ||B v - lambda v||: y'y on warp 0, y'Bv on warp 1 and, for the
+  // first iteration's sign, y'x on warp 2; then warp 0 normalises while warp 1
+  // forms the quotient and the residual.
+  if (warp < 3) {
+    dd acc{0, 0};
     double sgn = 0.0;
     for (int i = lane; i < n; i += 32) {
-      nrm = dd_add(nrm, dd_two_prod(y[i], y[i]));
-      num = dd_add(num, dd_two_prod(y[i], Bv[i]));
-      if (branch == 2) sgn = fma(y[i], x[i], sgn);
+      if (warp == 2)
+        sgn = branch == 2 ? fma(y[i], x[i], sgn) : 0.0;
+      else
+        acc = dd_add(acc, dd_two_prod(y[i], warp == 0 ? y[i] : Bv[i]));
     }
-    nrm = warp_sum_dd(nrm);
-    num = warp_sum_dd(num);
-    sgn = warp_sum(sgn);
-    const dd rq = dd_div(num, nrm);
-    const double lam = dd_to_d(rq);
-    const double flip = (branch == 1) ? (y[0] < 0.0 ? -1.0 : 1.0) : (sgn < 0.0 ? -1.0 : 1.0);
+    if (warp == 2) {
+      sgn = warp_sum(sgn);
+      if (lane == 0) s_sgn = sgn;
+    } else {
+      acc = warp_sum_dd(acc);
+      if (lane == 0) s_sum3[warp] = acc;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const dd nrm = s_sum3[0];
+    const double flip = (branch == 1) ? (y[0] < 0.0 ? -1.0 : 1.0) : (s_sgn < 0.0 ? -1.0 : 1.0);
     const dd inv = dd_div(dd{flip, 0.0}, dd_sqrt(nrm));
-    double acc = 0.0;
     for (int i = lane; i < n; i += 32) {
       const dd vi = dd_mul_d(inv, y[i]);
       vhi[i] = vi.hi;
       vlo[i] = vi.lo;
+    }
+  } else if (warp == 1) {
+    const dd nrm = s_sum3[0];
+    const dd rq = dd_div(s_sum3[1], nrm);
+    const double lam = dd_to_d(rq);
+    double acc = 0.0;
+    for (int i = lane; i < n; i += 32) {
       const double t = fma(-lam, y[i], Bv[i]);
       acc = fma(t, t, acc);
     }

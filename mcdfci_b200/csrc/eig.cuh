@@ -1140,45 +1140,45 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
 //    which contracts by about max_i sum_j |E_ij| / (d_i - lambda) per step, less
 //    than 1 whenever lambda < g (C is strongly diagonal in a subspace of picked
 //    determinants, most of which are not connected by a single or double
-//    excitation).  Lane l holds rows l and l + 32 and their y in registers; a
-//    step's product E y takes y_j from lane j by a shuffle, over each row's
-//    nonzeros (at most kBorderPack of them, kept in registers) or, when some
-//    row has more, over every column.  The division by d_i - lambda is one
-//    Newton-Raphson step of the reciprocal, r <- r + r e with e = 1 - (d_i -
-//    lambda) r, from the last step's r, while |e| < 1e-3 (lambda moves less
-//    every step, so the error falls quadratically), and a division otherwise
-//    (the first steps); an inexact r changes only the step, not the fixed
-//    point.
-//    The product also gives the residual of the current iterate exactly,
-//    r_i = (b + E y)_i + (d_i - lambda) y_i (row 0's is zero by the choice of
-//    lambda), so a step is one product, one warp reduction of three values and
-//    a few FMAs, with no block barrier, no shared-memory traffic, and no
-//    division or square root.  The iteration stops when ||r|| / ||v|| reaches
+//    excitation).  The product E y of a step also gives the residual of the
+//    current iterate, r_i = (b + E y)_i + (d_i - lambda) y_i (row 0's residual
+//    is zero by the choice of lambda), so a step costs one matrix-vector
+//    product, a reciprocal per row and one warp reduction of three values, with
+//    no block barrier.  The reciprocal of d_i - lambda is one Newton-Raphson
+//    step, r <- r + r e with e = 1 - (d_i - lambda) r, from the last step's r,
+//    while |e| < 1e-3 (lambda moves less every step, so the error falls
+//    quadratically), and a division otherwise (the first steps); an inexact r
+//    changes only the step, not the fixed point.  E is sparse (most picked determinants are not
+//    connected), so each lane first packs its rows' nonzero entries of E into
+//    `pack`, 2 (k + 1) lda doubles of scratch (values of row i from i lda on;
+//    after the k rows of values, their columns as 4-byte ints, row i from
+//    i (2 lda + 1) on), and a step's product runs over those only.  The
+//    iteration stops when ||r|| / ||v|| reaches
 //    1e-15 max_i sum_j |B_ij| (or stalls within 16 times that), and gives up
 //    when it stops contracting or lambda is not below g; A is only read.
 //    Returns true (uniform over the block) with V.y = (1, y) when the pair is
 //    certified; *iters receives the steps taken and *resid the final residual
-//    norm.  All threads call it; clk marks 17 (set-up), 18 (products), 19
-//    (reductions and tests) and 20 (the rest of a step).
+//    norm.  All threads call it.
 constexpr int kBorderMaxK = 64;
 constexpr int kBorderIters = 64;
-constexpr int kBorderPack = 6;
 
-__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, int* iters, double* resid,
-                                    SectionClock& clk) {
+__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, double* pack, int* iters,
+                                    double* resid, SectionClock& clk) {
   __shared__ int s_ok, s_it;
   __shared__ double s_rn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int k = n - 1;
   if (warp == 0) {
-    const bool two = k > 32;  // rows 32.. in the second register set
+    double* ys = V.y + 1;  // y_j at ys[j]
     const double a = A[0];
-    double d[2], b[2], y[2], rcp[2];
-    double pv[2][kBorderPack];
-    int pc[2][kBorderPack];
+    double d[2], b[2], y[2];
     bool own[2];
     int cnt[2];
     double gl = 1e300, nb = 0.0, babs = 0.0;
+    // Row i's nonzero off-diagonal entries of C: values at pv + i lda, their
+    // columns at pc + i (2 lda + 1) (an odd stride in 4-byte words).
+    double* const pv = pack;
+    int* const pc = reinterpret_cast<int*>(pack + static_cast<size_t>(k) * lda);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int i = lane + 32 * q;
@@ -1186,111 +1186,84 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
       const double* row = A + (i + 1) * lda + 1;
       d[q] = own[q] ? row[i] : 0.0;
       b[q] = own[q] ? A[i + 1] : 0.0;
-#pragma unroll
-      for (int p = 0; p < kBorderPack; ++p) {
-        pv[q][p] = 0.0;
-        pc[q][p] = lane;
-      }
       double off = 0.0;
       int c = 0;
-      if (own[q]) {
-        for (int j0 = 0; j0 < k; j0 += 8) {
-          double v[8];
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) v[jj] = j0 + jj < k ? row[j0 + jj] : 0.0;
-#pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            const int j = j0 + jj;
-            if (j != i && v[jj] != 0.0) {
-              off += fabs(v[jj]);
-#pragma unroll
-              for (int p = 0; p < kBorderPack; ++p)
-                if (c == p) {
-                  pv[q][p] = v[jj];
-                  pc[q][p] = j;
-                }
-              ++c;
-            }
+      if (own[q])
+        for (int j = 0; j < k; ++j) {
+          const double v = row[j];
+          if (j != i && v != 0.0) {
+            off += fabs(v);
+            pv[i * lda + c] = v;
+            pc[i * (2 * lda + 1) + c] = j;
+            ++c;
           }
         }
+      cnt[q] = c;
+      y[q] = 0.0;
+      if (own[q]) {
         gl = fmin(gl, d[q] - off);
         nb = fmax(nb, fabs(d[q]) + off + fabs(b[q]));
         babs += fabs(b[q]);
+        ys[i] = 0.0;
       }
-      cnt[q] = c;
-      y[q] = 0.0;
     }
+    int cmax = max(cnt[0], cnt[1]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       gl = fmin(gl, __shfl_xor_sync(~0u, gl, o));
       nb = fmax(nb, __shfl_xor_sync(~0u, nb, o));
       babs += __shfl_xor_sync(~0u, babs, o);
+      cmax = max(cmax, __shfl_xor_sync(~0u, cmax, o));
     }
     nb = fmax(nb, fabs(a) + babs);
-    const bool dense = __any_sync(~0u, cnt[0] > kBorderPack || cnt[1] > kBorderPack);
+    if (lane == 0) V.y[0] = 1.0;
+    __syncwarp();
+    clk.mark(17);
     const double tol = 1e-15 * nb;
     const double tol2 = tol * tol;
     double lam = fmin(a, gl) - 1e-3 * (1.0 + fabs(a));
+    double rcp[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) rcp[q] = own[q] ? 1.0 / (d[q] - lam) : 0.0;
-    clk.mark(17);
-    // The tests compare squared residual norms |r|^2 / |v|^2 cross-multiplied.
+    // The tests compare squared residual norms |r|^2 / |v|^2 cross-multiplied,
+    // so that no division or square root sits on a step's chain.
     double rrp = 1e300, vvp = 1.0;  // |r|^2 and |v|^2 of the previous step
     bool ok = false;
     int t = 0;
     for (; t < kBorderIters; ++t) {
-      // s = b + E y_t for this lane's rows.
-      double s0[2] = {0.0, 0.0}, s1[2] = {0.0, 0.0};
-      if (!dense) {
-#pragma unroll
-        for (int p = 0; p < kBorderPack; ++p) {
-#pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            if (q == 1 && !two) continue;
-            const int c = pc[q][p];
-            double yv = __shfl_sync(~0u, y[0], c & 31);
-            if (two) {
-              const double y1 = __shfl_sync(~0u, y[1], c & 31);
-              yv = c < 32 ? yv : y1;
-            }
-            if (p & 1)
-              s1[q] = fma(pv[q][p], yv, s1[q]);
-            else
-              s0[q] = fma(pv[q][p], yv, s0[q]);
-          }
-        }
-      } else {
-        const double* r0 = A + (lane + 1) * lda + 1;
-        const double* r1 = A + (lane + 33) * lda + 1;
-        for (int j = 0; j < k; ++j) {
-          const double yv = j < 32 ? __shfl_sync(~0u, y[0], j) : __shfl_sync(~0u, y[1], j - 32);
-          if (own[0] && j != lane) {
-            if (j & 1)
-              s1[0] = fma(r0[j], yv, s1[0]);
-            else
-              s0[0] = fma(r0[j], yv, s0[0]);
-          }
-          if (two && own[1] && j != lane + 32) {
-            if (j & 1)
-              s1[1] = fma(r1[j], yv, s1[1]);
-            else
-              s0[1] = fma(r1[j], yv, s0[1]);
-          }
-        }
-      }
+      // s = b + E y_t for this lane's rows, over their packed nonzeros.
       double s[2], yn[2];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        s[q] = b[q] + (s0[q] + s1[q]);
-        if (t > 0) {
-          const double x = d[q] - lam;
-          const double e = fma(-x, rcp[q], 1.0);  // relative error of rcp as 1 / x
-          if (fabs(e) < 1e-3)
-            rcp[q] = fma(rcp[q], e, rcp[q]);
-          else
-            rcp[q] = 1.0 / x;
+        const int i = lane + 32 * q;
+        const double* rv = pv + i * lda;
+        const int* rc = pc + i * (2 * lda + 1);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (q == 0 || k > 32) {
+          const int c = cnt[q];
+          int e = 0;
+          for (; e + 3 < cmax; e += 4) {
+            if (e < c) s0 = fma(rv[e], ys[rc[e]], s0);
+            if (e + 1 < c) s1 = fma(rv[e + 1], ys[rc[e + 1]], s1);
+            if (e + 2 < c) s2 = fma(rv[e + 2], ys[rc[e + 2]], s2);
+            if (e + 3 < c) s3 = fma(rv[e + 3], ys[rc[e + 3]], s3);
+          }
+          for (; e < cmax; ++e)
+            if (e < c) s0 = fma(rv[e], ys[rc[e]], s0);
+          s[q] = b[q] + ((s0 + s1) + (s2 + s3));
+          if (t > 0) {
+            const double x = d[q] - lam;
+            const double e = fma(-x, rcp[q], 1.0);  // relative error of rcp as 1 / x
+            if (fabs(e) < 1e-3)
+              rcp[q] = fma(rcp[q], e, rcp[q]);
+            else
+              rcp[q] = 1.0 / x;
+          }
+          yn[q] = own[q] ? -s[q] * rcp[q] : 0.0;
+        } else {
+          s[q] = 0.0;
+          yn[q] = 0.0;
         }
-        yn[q] = own[q] ? -s[q] * rcp[q] : 0.0;
       }
       clk.mark(18);
       // Residual of (lambda_t, v_t), |y_t|^2 and b'y_{t+1}, in one reduction.
@@ -1325,17 +1298,17 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
       clk.mark(19);
       rrp = rr;
       vvp = vv;
-      y[0] = yn[0];
-      y[1] = yn[1];
+      __syncwarp();  // every lane has read y_t
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        y[q] = yn[q];
+        if (own[q]) ys[lane + 32 * q] = yn[q];
+      }
       lam = a + by;
+      __syncwarp();
       clk.mark(20);
     }
-    // V.y = (1, y_t), the iterate whose residual was taken.
-#pragma unroll
-    for (int q = 0; q < 2; ++q)
-      if (own[q]) V.y[1 + lane + 32 * q] = y[q];
     if (lane == 0) {
-      V.y[0] = 1.0;
       s_ok = ok;
       s_it = t + 1;
     }

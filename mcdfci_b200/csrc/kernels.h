@@ -152,9 +152,9 @@ struct RdmLaunch {
 // 16 the fast solver of eig_method 1 or 2 (when it runs, in place of 10-13:
 // its set-up and, when it fails, the restore), the rest of it in 17-20:
 // method 1: 17 Cholesky factorisation, 18 explicit inverse, 19 power steps,
-// 20 refinement steps; method 2: 17 set-up (H_sub's nonzeros into registers,
-// the bounds), 18 products of its steps, 19 their reductions and tests, 20
-// the rest of each step.  The eig set-up (9) is split further: 21 H_sub into
+// 20 refinement steps; method 2: 17 set-up (packing of H_sub's nonzeros, the
+// bounds), 18 products and reciprocals of its steps, 19 their reductions and
+// tests, 20 their stores.  The eig set-up (9) is split further: 21 H_sub into
 // B, 22 H x, 23 the double-double sums of x'x, x'z, x'Hx (9 is then the first
 // row of B), and the Rayleigh quotient (14): 24 the product B v (14 is then
 // the double-double quotient, normalisation and residual).

@@ -244,18 +244,18 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   }
   __syncthreads();
   clk.mark(22);
-  // The three sums on warps 0, 1, 2 (each in the same order as alone).
-  if (warp < 3) {
-    const double* w = warp == 0 ? x : (warp == 1 ? z : Hx);
-    dd acc{0, 0};
-    for (int i = lane; i < k; i += 32) acc = dd_add(acc, dd_two_prod(x[i], w[i]));
-    acc = warp_sum_dd(acc);
-    if (lane == 0) s_sum3[warp] = acc;
-  }
-  __syncthreads();
   if (warp == 0) {
+    dd sxx{0, 0}, sxz{0, 0}, sxhx{0, 0};
+    for (int i = lane; i < k; i += 32) {
+      sxx = dd_add(sxx, dd_two_prod(x[i], x[i]));
+      sxz = dd_add(sxz, dd_two_prod(x[i], z[i]));
+      sxhx = dd_add(sxhx, dd_two_prod(x[i], Hx[i]));
+    }
+    sxx = warp_sum_dd(sxx);
+    sxz = warp_sum_dd(sxz);
+    sxhx = warp_sum_dd(sxhx);
     if (lane == 0) {
-      const double xTx = dd_to_d(s_sum3[0]), xTz = dd_to_d(s_sum3[1]), xTHx = dd_to_d(s_sum3[2]);
+      const double xTx = dd_to_d(sxx), xTz = dd_to_d(sxz), xTHx = dd_to_d(sxhx);
       const double yy = dd_to_d(dd_add_d(xx, -xTx));
       s_branch = fabs(yy) > 1e-14 ? 1 : 2;
       if (s_branch == 1) {
@@ -309,7 +309,7 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   if (!shifted && method == 2 && branch == 1 && k <= kBorderMaxK) {
     int iters = 0;
     double rn = 0.0;
-    bordered = eig_lowest_bordered(A, lda, n, V, &iters, &rn, clk);
+    bordered = eig_lowest_bordered(A, lda, n, V, Li, &iters, &rn, clk);  // Li and Ci as its scratch
     res.shift_steps = bordered ? iters : 0;
     res.shift_diff = rn;
     res.fallback = !bordered;

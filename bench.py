@@ -807,6 +807,8 @@ def e2e_run(mc, fc, args, local_rank):
         "create_device_alloc_ms": stages["device_alloc"],
         "create_upload_ms": stages["upload"],
         "create_device_setup_ms": stages["device_setup"],
+        "create_upload_copy_ms": stages["upload_copy"],
+        "create_upload_sync_ms": stages["upload_sync"],
         "solve_ms": 1000.0 * dt - create_ms,
         "solve_table_fill_ms": stages["table_fill"],
         "solve_graph_build_ms": stages["graph_build"],

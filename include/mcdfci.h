@@ -330,11 +330,13 @@ int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied);
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
 /* The hash table: slots now, slots at full size (max_memory), growths so far. */
 int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_capacity, int32_t* growths);
-/* Host wall time of the solver's set-up stages in milliseconds, up to n of
- * them: 0 Hamiltonian tables and reference determinant (host), 1 device
- * allocations at creation, 2 table upload, 3 table fill of the last reset
- * (synchronised), 4 CUDA graph builds, 5 table growths, 6 report read-backs,
- * 7 device and stream set-up, summed since creation.  No counterpart in the
+/* Host wall time of the solver's set-up stages in milliseconds, up to n
+ * (<= 10) of them: 0 Hamiltonian tables (host, on a host thread during 7 and
+ * 1), 1 device allocations at creation, 2 the wait for the host tables and
+ * their upload, 3 table fill of the last reset (synchronised), 4 CUDA graph
+ * builds, 5 table growths, 6 report read-backs, 7 device and stream set-up,
+ * 8 and 9 parts of 2 (the copy into pinned staging, the final stream
+ * synchronisation), summed since creation.  No counterpart in the
  * reference. */
 int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n);
 /* The autotuner's record: the fixed rule's CTAs per column, the chosen

@@ -485,7 +485,7 @@ class CDFCI:
         return h.reshape(k, k)
 
     SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports",
-                    "device_setup")
+                    "device_setup", "upload_copy", "upload_sync")
 
     def autotune_info(self) -> dict:
         rule, chosen, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

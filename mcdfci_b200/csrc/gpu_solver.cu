@@ -562,8 +562,10 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
       add(o_sp, ham_.spres.data(), n_sp * 8);
       add(o_vss, ham_.vss.data(), n_vss * 8);
       add(o_wab, ham_.wab.data(), n_wab * 8);
+      const auto t_copy = clock::now();
       host_parallel(static_cast<int>(pieces.size()),
                     [&](int i) { std::memcpy(st + pieces[i].dst, pieces[i].src, pieces[i].bytes); });
+      setup_ms_[8] = ms_since(t_copy);
       check(cudaMemcpyAsync(base, st, off, cudaMemcpyHostToDevice, stream_), "upload tables");
     } else {
       up(o_hd, ham_.hdiag.data(), n_hd * 8);
@@ -614,7 +616,9 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
   ll_.eig_method = opt_.eig_method;
+  const auto t_sync = clock::now();
   const cudaError_t sync_err = cudaStreamSynchronize(stream_);
+  setup_ms_[9] = ms_since(t_sync);
   staging_release(stage);
   check(sync_err, "table upload");
   setup_ms_[1] = alloc_ms;

@@ -132,8 +132,10 @@ class GpuSolver {
   // after 1 and their upload, 3 table fill of the last
   // reset (synchronised), 4 CUDA graph builds, 5 table growths, 6 report
   // read-backs (finish, state copy, synchronisation), 7 device and stream
-  // set-up (device, stream, attributes, free memory), summed since creation.
-  static constexpr int kSetupStages = 8;
+  // set-up (device, stream, attributes, free memory), summed since creation;
+  // 8 and 9 are parts of 2: the copy of the tables into pinned staging and
+  // the constructor's final synchronisation with the stream.
+  static constexpr int kSetupStages = 10;
   const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }

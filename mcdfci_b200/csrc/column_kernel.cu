@@ -228,12 +228,6 @@ __device__ __forceinline__ bool above_threshold(dd scale, double dz, double zt) 
   return dd_gt(dd_abs(dd_mul_d(scale, dz)), dd{zt, 0.0});
 }
 
-__device__ __forceinline__ double score_of(double x, double z, dd xss) {
-  if (x == 0.0) return fabs(z);
-  const dd t = dd_add_d(dd_mul_d(xss, x), z);
-  return fabs(t.hi + t.lo);
-}
-
 // ---------------------------------------------------------------------------
 
 // Merges a descending list stored in global memory by another CTA (read

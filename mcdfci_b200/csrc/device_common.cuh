@@ -217,6 +217,14 @@ __device__ __forceinline__ long long table_upsert(const TableDev& t, uint64_t a,
   return table_upsert_from(t, a, b, i, ka, kb, inserted);
 }
 
+// gcd_grad score of a determinant, |x xx scale^2 + z| (CoordinatePickGcdGrad,
+// src/solver.h:118-143), with xss = xx scale^2 in double-double.
+__device__ __forceinline__ double score_of(double x, double z, dd xss) {
+  if (x == 0.0) return fabs(z);
+  const dd t = dd_add_d(dd_mul_d(xss, x), z);
+  return fabs(t.hi + t.lo);
+}
+
 // ---------------------------------------------------------------------------
 // Section clock: thread 0 of a CTA adds the SM cycles since the previous mark
 // to acc[i].  Marks are placed right after block-wide barriers, so each entry

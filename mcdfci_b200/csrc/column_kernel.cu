@@ -408,11 +408,7 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk, cons
     toplist_offer<R>(T, key, slotu);
     if (timed) t_off += clock64() - q3;
   }
-  if (MODE == kColProbe) {
-    // The CTA's next block rebuilds P: every warp must be done with this one.
-    __syncthreads();
-    return;
-  }
+  if (MODE == kColProbe) return;
   const long long c_post = timed ? clock64() : 0;
   if (timed) {
     atomicAdd(L.sect + 0, t_gen);

@@ -93,8 +93,6 @@ def parse_args():
                     help="print where the device time of an iteration goes (leader and column phase timers) "
                          "on --phase-workload instead of the bench line")
     ap.add_argument("--phase-workload", default="n24_6a6b")
-    ap.add_argument("--fused", type=int, default=1, choices=[0, 1],
-                    help="1: one fused cooperative launch per iteration (the library's default); 0: two kernels")
     ap.add_argument("--eig-method", type=int, default=2, choices=[0, 1, 2],
                     help="subspace eigenproblem: 1 shifted inverse iteration first, 0 the full reduction")
     ap.add_argument("--scatter-sweep", action="store_true",
@@ -403,7 +401,7 @@ def phases_arm(args, local_rank):
         synth.write_fcidump(path, args.phase_workload, seed=args.seed)
         s = mc.CDFCI(mc.Fcidump(path), num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                      z_threshold=args.z_threshold, threshold=0.0, groups=args.groups, device=local_rank,
-                     eig_method=args.eig_method, num_iterations=args.warmup + args.steps, fused=args.fused)
+                     eig_method=args.eig_method, num_iterations=args.warmup + args.steps)
         s.reset()
         s.run_iterations(args.warmup)
         rb = s.report()
@@ -635,8 +633,7 @@ def b200_arm(args, rank, world, local_rank):
         # sized for them, up to two 64-iteration chunks).
         solver = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                           z_threshold=args.z_threshold, threshold=0.0, device=local_rank, groups=args.groups,
-                          num_iterations=args.warmup + 2 * args.steps + max(args.aged_iterations, 0) + args.aged_steps,
-                          fused=args.fused)
+                          num_iterations=args.warmup + 2 * args.steps + max(args.aged_iterations, 0) + args.aged_steps)
         solver.reset()
         solver.run_iterations(args.warmup)
         r0 = solver.report()
@@ -789,13 +786,13 @@ def e2e_run(mc, fc, args, local_rank):
     wpath = os.path.join(os.path.dirname(fc.path), "warmup_n7.fcidump")
     synth.write_fcidump(wpath, "n7_5a5b", seed=0)
     w = mc.CDFCI(mc.Fcidump(wpath), num_of_coordinate=args.k, estimate=args.m, max_memory=0.001,
-                 threshold=0.0, device=local_rank, num_iterations=10, report_interval=5, fused=args.fused)
+                 threshold=0.0, device=local_rank, num_iterations=10, report_interval=5)
     w.solve()
     w.close()
     t0 = time.perf_counter()
     s = mc.CDFCI(fc, num_of_coordinate=args.k, estimate=args.m, max_memory=args.max_memory,
                  z_threshold=args.z_threshold, threshold=0.0, device=local_rank, num_iterations=iters,
-                 report_interval=interval, groups=args.groups, fused=args.fused)
+                 report_interval=interval, groups=args.groups)
     t_created = time.perf_counter()
     s.solve()
     energy = s.result_energy

@@ -118,17 +118,8 @@ typedef struct mcd_options {
    * (the trials are iterations of the solve), among values around the fixed
    * rule's, the fastest column kernel kept and remembered for the process
    * per (orbitals, electrons, k, m, SM count).  0 (default): the fixed rule.
-   * Not used with the fused iteration.  No counterpart in the reference. */
+   * No counterpart in the reference. */
   int32_t autotune;
-  /* 1 (default): each iteration is one cooperative launch of one 512-thread
-   * CTA per SM: CTA 0 runs the leader (pick, H_sub, eigenproblem), the others
-   * generate the picked columns and probe the table while the eigenproblem
-   * is solved, then apply z += H dx and keep the candidates once dx is
-   * known; when the device supports cooperative launches and the probe
-   * records (32 bytes per column entry) stay within 256 MB.  0: the leader
-   * and column kernels one after the other.  Same results either way.  No
-   * counterpart in the reference. */
-  int32_t fused;
 } mcd_options;
 
 /* One line of the reference's report table (src/solver.h:761-798). */
@@ -398,10 +389,6 @@ int mcd_debug_column_sections(mcd_solver* s, uint64_t* cycles, int32_t n, int32_
  * *n_out receives the count.  No counterpart in the reference. */
 int mcd_debug_slots(mcd_solver* s, uint64_t* alpha, uint64_t* beta, double* x, double* z, int64_t cap,
                     int64_t* n_out);
-/* Whether the solver runs the fused iteration (mcd_options.fused), with its
- * CTAs per launch and column blocks (of 512 threads) per column.  No
- * counterpart in the reference. */
-int mcd_debug_fused_info(const mcd_solver* s, int32_t* fused, int32_t* ctas, int32_t* blocks_per_column);
 /* The inputs of the last iteration's subspace eigenproblem, the arguments of
  * CoordinateUpdateEig::operator() (src/solver.h:333-345): H_sub (k x k,
  * row-major), the picked coordinates' x and z before the update, and the

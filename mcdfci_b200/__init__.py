@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "mcd_create", "mcd_create_from_fcidump", "mcd_destroy", "mcd_solve", "mcd_reset",
     "mcd_run_iterations", "mcd_run_iterations_timed", "mcd_get_report", "mcd_result", "mcd_stream", "mcd_scalars",
     "mcd_last_error", "mcd_run_json", "mcd_debug_column", "mcd_debug_hsub", "mcd_debug_eig",
-    "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_last_eig", "mcd_debug_fused_info", "mcd_debug_launch_info", "mcd_debug_leader_sections",
+    "mcd_debug_table_sums", "mcd_debug_picked", "mcd_debug_last_eig", "mcd_debug_launch_info", "mcd_debug_leader_sections",
     "mcd_debug_scatter_rate",
     "mcd_eig_update_static",
     "mcd_batch_create", "mcd_batch_destroy", "mcd_batch_size", "mcd_batch_solve", "mcd_batch_reset",
@@ -79,7 +79,6 @@ class mcd_options(ctypes.Structure):
         ("groups", ctypes.c_int32), ("verbose", ctypes.c_int32),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int32), ("compaction", ctypes.c_int32),
         ("table_growth", ctypes.c_int32), ("eig_method", ctypes.c_int32), ("autotune", ctypes.c_int32),
-        ("fused", ctypes.c_int32),
     ]
 
 
@@ -166,8 +165,6 @@ def library() -> ctypes.CDLL:
     L.mcd_debug_table_sums.argtypes = [vp, _dp, _dp, _u64p]
     L.mcd_debug_picked.argtypes = [vp, _u64p, _u64p, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     L.mcd_debug_last_eig.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
-    L.mcd_debug_fused_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
-                                       ctypes.POINTER(ctypes.c_int32)]
     i32p = ctypes.POINTER(ctypes.c_int32)
     L.mcd_debug_launch_info.argtypes = [vp, i32p, i32p, i32p]
     L.mcd_debug_scatter_rate.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
@@ -301,7 +298,7 @@ def make_options(**kw) -> mcd_options:
     """mcd_options with the reference defaults, then keyword overrides
     (num_iterations, report_interval, num_of_coordinate, estimate, z_threshold,
     z_threshold_search, max_memory, threshold, ref_det_occ, coordinate_update
-    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth, eig_method, autotune, fused)."""
+    ("eig"|"ls"), groups, verbose, stream, device, compaction, table_growth, eig_method)."""
     o = mcd_options()
     library().mcd_options_default(ctypes.byref(o))
     occ = kw.pop("ref_det_occ", None)
@@ -315,7 +312,7 @@ def make_options(**kw) -> mcd_options:
             o.z_threshold_search = int(bool(v))
         elif k == "eig_method":
             o.eig_method = int(v)
-        elif k in ("compaction", "table_growth", "autotune", "fused"):
+        elif k in ("compaction", "table_growth", "autotune"):
             setattr(o, k, int(bool(v)))
         else:
             setattr(o, k, v)
@@ -562,12 +559,6 @@ class CDFCI:
         _check(library().mcd_debug_scatter_rate_mode(self._h, int(entries), int(reps), int(ilp), int(ctas_per_sm),
                                                      int(mode), ctypes.byref(r)))
         return r.value
-
-    def fused_info(self) -> dict:
-        """Whether the fused iteration runs, its CTAs and blocks per column."""
-        f, c, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        _check(library().mcd_debug_fused_info(self._h, ctypes.byref(f), ctypes.byref(c), ctypes.byref(g)))
-        return {"fused": bool(f.value), "ctas": c.value, "blocks_per_column": g.value}
 
     def launch_info(self) -> dict:
         c, mac, e = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

@@ -75,7 +75,6 @@ mcd::SolverOptions to_options(const mcd_options* o) {
   if (o->eig_method < 0 || o->eig_method > 2) throw mcd::McdError(MCD_ERR_INVALID, "eig_method must be 0, 1 or 2.");
   s.eig_method = o->eig_method;
   s.autotune = o->autotune != 0;
-  s.fused = o->fused != 0;
   s.verbose = o->verbose != 0;
   s.stream = static_cast<cudaStream_t>(o->stream);
   s.device = o->device;
@@ -162,7 +161,6 @@ void options_from_json(const mcd::Json& option, mcd_options* o, std::vector<int3
   if (cd.has("table_growth")) o->table_growth = cd.at("table_growth").as_bool("table_growth") ? 1 : 0;
   if (cd.has("eig_method")) o->eig_method = static_cast<int32_t>(cd.at("eig_method").as_number("eig_method"));
   if (cd.has("autotune")) o->autotune = cd.at("autotune").as_bool("autotune") ? 1 : 0;
-  if (cd.has("fused")) o->fused = cd.at("fused").as_bool("fused") ? 1 : 0;
   const std::string pick = cd.at("coordinate_pick").as_string("coordinate_pick");
   const std::string upd = cd.at("coordinate_update").as_string("coordinate_update");
   if (pick != "gcd_grad") throw mcd::McdError(MCD_ERR_INVALID, "the coordinate pick method \"" + pick + "\" is not implemented.");
@@ -201,7 +199,6 @@ void mcd_options_default(mcd_options* o) {
   o->table_growth = 1;
   o->eig_method = 2;
   o->autotune = 0;
-  o->fused = 1;
   o->verbose = 0;
   o->stream = nullptr;
   o->device = -1;
@@ -781,16 +778,6 @@ int mcd_debug_launch_info(mcd_solver* s, int32_t* groups, int32_t* list_size, in
     if (groups) *groups = s->impl->groups();
     if (list_size) *list_size = s->impl->list_size();
     if (entries) *entries = s->impl->entries_per_column();
-    return MCD_OK;
-  });
-}
-
-int mcd_debug_fused_info(const mcd_solver* s, int32_t* fused, int32_t* ctas, int32_t* blocks_per_column) {
-  return guarded([&] {
-    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
-    if (fused) *fused = s->impl->fused() ? 1 : 0;
-    if (ctas) *ctas = s->impl->fused_ctas();
-    if (blocks_per_column) *blocks_per_column = s->impl->fused_groups();
     return MCD_OK;
   });
 }

@@ -41,11 +41,8 @@
 // dot products (summed in a fixed order).
 #include "device_common.cuh"
 #include <algorithm>
-#include <map>
-#include <mutex>
 
 #include "kernels.h"
-#include "leader_body.cuh"
 #include "toplist.cuh"
 
 namespace mcd {
@@ -252,29 +249,16 @@ __device__ __forceinline__ void toplist_merge_global(TopList<R>& L, const unsign
   bitonic_merge_desc<R>(L);
 }
 
-// Modes of column_body: the whole update (the column kernels), or its two
-// halves in the fused iteration kernel: the generation and probes, which need
-// only the picked determinants, and, once dx is known, the z updates, the
-// candidates and the merge.
-enum ColumnMode { kColFull = 0, kColProbe = 1, kColUpdate = 2 };
-
-// Double-double from two doubles read through L2 (values another CTA of the
-// same launch published).
-__device__ __forceinline__ dd ldcg_dd(const dd* p) { return dd{__ldcg(&p->hi), __ldcg(&p->lo)}; }
-
-// One block's share of one column: block `blk` of the launch described by L
-// (column blk / groups, slice blk % groups), NT threads (the whole CTA).  In
-// kColProbe and kColUpdate mode `rec` holds the probe results (EntryRecords).
-template <int R, int NT = kNT, int MODE = kColFull>
-__device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk, const EntryRecords* rec = nullptr) {
+// One CTA's share of one column: CTA `blk` of the launch described by L
+// (column blk / groups, slice blk % groups).
+template <int R>
+__device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   constexpr int M = 32 * R;
-  constexpr int kW = NT / 32;
-  constexpr bool kPublished = MODE != kColFull;  // iteration state written by another CTA of this launch
   const int G = L.groups;
   const int col = blk / G;
   const int g = blk - col * G;
   IterState* S = L.st;
-  const int kcur = kPublished ? __ldcg(&S->k_cur) : S->k_cur;
+  const int kcur = S->k_cur;
   if (col >= kcur) return;
 
   __shared__ Prelude P;
@@ -287,25 +271,20 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk, cons
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool timed = L.sect != nullptr && threadIdx.x == 0;
   const long long c_start = timed ? clock64() : 0;
-  // The column's scalars are read while warp 0 decodes the determinant (in
-  // the probe phase dx and H_cc are not known yet and not used).
-  const double dxc = MODE == kColProbe ? 0.0 : (kPublished ? __ldcg(&S->dx[col]) : S->dx[col]);
-  const double hd = MODE == kColProbe ? 0.0 : (kPublished ? __ldcg(&S->hdiag[col]) : S->hdiag[col]);
-  const dd xss = kPublished ? ldcg_dd(&S->xss) : S->xss;
-  const dd scale = kPublished ? ldcg_dd(&S->scale) : S->scale;
+  // The column's scalars are read while warp 0 decodes the determinant.
+  const double dxc = S->dx[col];
+  const double hd = S->hdiag[col];
+  const dd xss = S->xss;
+  const dd scale = S->scale;
   const dd zt{S->zt, 0.0};
-  const unsigned dslot = static_cast<unsigned>(kPublished ? __ldcg(&S->slot[col]) : S->slot[col]);
-  if (MODE != kColUpdate && warp == 0) {
-    const Det d = kPublished ? Det{__ldcg(&S->det[col].a), __ldcg(&S->det[col].b)} : S->det[col];
-    build_prelude(P, d, L.ham.norb);
-  }
-  if (MODE == kColUpdate && threadIdx.x == 0) P.total = static_cast<int>(rec->per_col);
+  const unsigned dslot = static_cast<unsigned>(S->slot[col]);
+  if (warp == 0) build_prelude(P, S->det[col], L.ham.norb);
   __syncthreads();
   const int total = P.total;
   const int per = (total + G - 1) / G;
   const int beg = min(total, g * per);
   const int end = min(total, beg + per);
-  const int nrounds = (end - beg + NT - 1) / NT;
+  const int nrounds = (end - beg + kNT - 1) / kNT;
 
   TopList<R> T;
   toplist_clear<R>(T);
@@ -316,91 +295,47 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk, cons
   const long long c_rounds = timed ? clock64() : 0;
   for (int r = 0; r < nrounds; ++r) {
     long long q0 = timed ? clock64() : 0;
-    const int e = beg + r * NT + threadIdx.x;
+    const int e = beg + r * kNT + threadIdx.x;
     unsigned long long key = 0ull;
     unsigned slotu = 0u;
-    if (MODE == kColProbe) {
-      // Generation and probe only: what the update will need, per entry.
-      if (e < end) {
-        uint64_t a2, b2;
-        double v;
-        const int kind = gen_entry(L.ham, P, e, 0.0, a2, b2, v);
-        long long code = kRecSkip;
-        if (kind != kNone && (kind == kKeep || v != 0.0)) {
-          const uint64_t home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
-          uint64_t ka = 0, kb = 0;
-          load_key(L.tab.slots + home, ka, kb);
-          code = table_find_pos_from(L.tab, a2, b2, home, ka, kb);
-        }
-        const size_t ri = static_cast<size_t>(col) * rec->per_col + e;
-        rec->v[ri] = v;
-        rec->code[ri] = code;
-        rec->a[ri] = a2;
-        rec->b[ri] = b2;
-      }
-      continue;
-    }
     if (e < end) {
-      uint64_t a2 = 0, b2 = 0, ka = 0, kb = 0;
-      double v = 0.0;
-      bool keep = false;
-      uint64_t home = 0;
-      long long found = -1;  // kColUpdate: the slot the probe found
-      if (MODE == kColFull) {
-        const int kind = gen_entry(L.ham, P, e, hd, a2, b2, v);
-        if (kind != kNone) {
-          // Start the probe at the home slot before the integral value is used
-          // (the diagonal entry's slot is the picked determinant's own).
-          home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
-          load_key(L.tab.slots + home, ka, kb);
-          keep = kind == kKeep || v != 0.0;
-        }
-      } else {
-        const size_t ri = static_cast<size_t>(col) * rec->per_col + e;
-        const long long code = rec->code[ri];
-        keep = code != kRecSkip;
-        if (keep) {
-          v = e == 0 ? hd : rec->v[ri];
-          if (code >= 0) {
-            found = code;
-          } else {
-            // Absent at the probe: continue from the first empty slot it saw
-            // (another column may have inserted the determinant since).
-            a2 = rec->a[ri];
-            b2 = rec->b[ri];
-            home = static_cast<uint64_t>(-2 - code);
-            load_key(L.tab.slots + home, ka, kb);
-          }
-        }
-      }
-      long long q1 = 0;
-      if (timed) {
-        q1 = clock64();
-        t_gen += q1 - q0;
-      }
-      if (keep) {
-        ++emit;
-        const double dz = v * dxc;
-        bool inserted = false;
-        const long long slot =
-            found >= 0 ? found
-                       : table_probe_from(L.tab, a2, b2, home, ka, kb, above_threshold(scale, dz, zt.hi), inserted);
-        ins += inserted ? 1u : 0u;
-        long long q2 = 0;
+      uint64_t a2, b2;
+      double v;
+      const int kind = gen_entry(L.ham, P, e, hd, a2, b2, v);
+      if (kind != kNone) {
+        // Start the probe at the home slot before the integral value is used
+        // (the diagonal entry's slot is the picked determinant's own).
+        const uint64_t home = e == 0 ? static_cast<uint64_t>(dslot) : det_hash(a2, b2) & L.tab.mask;
+        uint64_t ka = 0, kb = 0;
+        load_key(L.tab.slots + home, ka, kb);
+        long long q1 = 0;
         if (timed) {
-          q2 = clock64();
-          t_probe += q2 - q1;
+          q1 = clock64();
+          t_gen += q1 - q0;
         }
-        if (slot >= 0) {
-          Slot* sp = L.tab.slots + slot;
-          const double x = kPublished ? load_relaxed(&sp->x) : sp->x;
-          const double znew = atomicAdd(&sp->z, dz) + dz;
-          ++upd;
-          acc_newz += v * x;
-          acc_dot += dz * x;
-          key = static_cast<unsigned long long>(__double_as_longlong(score_of(x, znew, xss))) + 1ull;
-          slotu = static_cast<unsigned>(slot);
-          if (timed) t_upd += clock64() - q2;
+        if (kind == kKeep || v != 0.0) {
+          ++emit;
+          const double dz = v * dxc;
+          bool inserted;
+          const long long slot =
+              table_probe_from(L.tab, a2, b2, home, ka, kb, above_threshold(scale, dz, zt.hi), inserted);
+          ins += inserted ? 1u : 0u;
+          long long q2 = 0;
+          if (timed) {
+            q2 = clock64();
+            t_probe += q2 - q1;
+          }
+          if (slot >= 0) {
+            Slot* sp = L.tab.slots + slot;
+            const double x = sp->x;
+            const double znew = atomicAdd(&sp->z, dz) + dz;
+            ++upd;
+            acc_newz += v * x;
+            acc_dot += dz * x;
+            key = static_cast<unsigned long long>(__double_as_longlong(score_of(x, znew, xss))) + 1ull;
+            slotu = static_cast<unsigned>(slot);
+            if (timed) t_upd += clock64() - q2;
+          }
         }
       }
     }
@@ -408,7 +343,6 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk, cons
     toplist_offer<R>(T, key, slotu);
     if (timed) t_off += clock64() - q3;
   }
-  if (MODE == kColProbe) return;
   const long long c_post = timed ? clock64() : 0;
   if (timed) {
     atomicAdd(L.sect + 0, t_gen);
@@ -564,68 +498,6 @@ __global__ void __launch_bounds__(kNT) debug_column_kernel(HamDev h, Det d, doub
         bo[pos] = b2;
         vo[pos] = v;
       }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Fused iteration: one cooperative launch of one 512-thread CTA per SM.  CTA 0
-// runs the leader; the others take the column blocks blk = cta - 1, cta - 1 +
-// (ctas - 1), ... twice: their generation and probes as soon as the leader
-// has published the picked determinants, their z updates, candidates and
-// merges once it has published dx.  The waits are thread 0's, on a
-// hand-over word of IterFlags, bounded by kFusedWaitCycles (about a second).
-constexpr int kFusedThreads = 512;
-constexpr long long kFusedWaitCycles = 2000000000ll;
-
-__device__ bool fused_wait(const unsigned long long* p, unsigned long long v, unsigned* err) {
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) {
-    int ok = 0;
-    const long long t0 = clock64();
-    for (;;) {
-      if (flag_acquire(p) >= v) {
-        ok = 1;
-        break;
-      }
-      if (clock64() - t0 > kFusedWaitCycles) break;
-      __nanosleep(128);
-    }
-    if (!ok) atomicOr(err, kErrWait);
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-template <int R>
-__global__ void __launch_bounds__(kFusedThreads, 1) fused_iteration_kernel(FusedLaunch F) {
-  __shared__ unsigned long long s_seq;
-  if (threadIdx.x == 0) s_seq = __ldcg(&F.flags->seq) + 1ull;
-  __syncthreads();
-  const unsigned long long seqno = s_seq;
-  if (blockIdx.x == 0) {
-    leader_body(F.lead, F.flags, seqno);
-  } else {
-    const int nblk = F.col.k_grid * F.col.groups;
-    const int step = static_cast<int>(gridDim.x) - 1;
-    if (fused_wait(&F.flags->picks, seqno, F.col.tab.err)) {
-      for (int blk = static_cast<int>(blockIdx.x) - 1; blk < nblk; blk += step)
-        column_body<R, kFusedThreads, kColProbe>(F.col, blk, &F.rec);
-      if (fused_wait(&F.flags->dx, seqno, F.col.tab.err))
-        for (int blk = static_cast<int>(blockIdx.x) - 1; blk < nblk; blk += step)
-          column_body<R, kFusedThreads, kColUpdate>(F.col, blk, &F.rec);
-    }
-  }
-  // The last CTA of the launch to finish advances the launch number (every
-  // CTA has read it by then).
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&F.flags->done, 1u) == gridDim.x - 1) {
-      F.flags->done = 0u;
-      __threadfence();
-      flag_release(&F.flags->seq, seqno);
     }
   }
 }
@@ -864,55 +736,6 @@ cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s) {
   if (a.m <= 32) return launch_column_r<1>(a, s);
   if (a.m <= 64) return launch_column_r<2>(a, s);
   return launch_column_r<4>(a, s);
-}
-
-namespace {
-template <int R>
-const void* fused_fn() {
-  return reinterpret_cast<const void*>(fused_iteration_kernel<R>);
-}
-const void* fused_kernel_for(int m) { return m <= 32 ? fused_fn<1>() : (m <= 64 ? fused_fn<2>() : fused_fn<4>()); }
-
-// Dynamic shared memory granted to the fused kernels, per device (the
-// leader's part needs more than the default 48 KB at large k and m).
-std::mutex g_fused_mu;
-std::map<int, size_t> g_fused_smem;
-
-cudaError_t fused_prepare(int m, size_t bytes) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  std::lock_guard<std::mutex> lock(g_fused_mu);
-  size_t& have = g_fused_smem[dev * 4 + (m <= 32 ? 0 : (m <= 64 ? 1 : 2))];
-  if (bytes <= have) return cudaSuccess;
-  e = cudaFuncSetAttribute(fused_kernel_for(m), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-  if (e == cudaSuccess) have = bytes;
-  return e;
-}
-}  // namespace
-
-int fused_fits(const FusedLaunch& f) {
-  const size_t bytes = leader_smem_bytes(f.lead.k_req, f.lead.m);
-  if (fused_prepare(f.lead.m, bytes) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return 0;
-  }
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fused_kernel_for(f.lead.m), kFusedThreads, bytes) !=
-      cudaSuccess) {
-    (void)cudaGetLastError();
-    return 0;
-  }
-  return n >= 1 ? 1 : 0;
-}
-
-cudaError_t launch_fused(const FusedLaunch& f, int ctas, cudaStream_t s) {
-  const size_t bytes = leader_smem_bytes(f.lead.k_req, f.lead.m);
-  cudaError_t e = fused_prepare(f.lead.m, bytes);
-  if (e != cudaSuccess) return e;
-  FusedLaunch arg = f;
-  void* args[] = {&arg};
-  return cudaLaunchCooperativeKernel(fused_kernel_for(f.lead.m), dim3(ctas), dim3(kFusedThreads), args, bytes, s);
 }
 
 cudaError_t launch_column_batch(const ColumnBatch& b, cudaStream_t s) {

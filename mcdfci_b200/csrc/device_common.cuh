@@ -151,21 +151,6 @@ __device__ __forceinline__ long long table_find_from(const TableDev& t, uint64_t
   return -1;
 }
 
-// Probe without inserting, continuing from a loaded home slot: the slot of
-// (a,b) (>= 0), or -2 - i with i the first empty slot of the run (where an
-// insert would go), or -1 (after raising kErrProbe) at the probe limit.
-__device__ __forceinline__ long long table_find_pos_from(const TableDev& t, uint64_t a, uint64_t b, uint64_t i,
-                                                         uint64_t ka, uint64_t kb) {
-  for (int p = 0; p < t.max_probe; ++p) {
-    if (p > 0) load_key(t.slots + i, ka, kb);
-    if (ka == a && kb == b) return static_cast<long long>(i);
-    if (ka == kEmptyKey && kb == kEmptyKey) return -2 - static_cast<long long>(i);
-    i = (i + 1) & t.mask;
-  }
-  atomicOr(t.err, kErrProbe);
-  return -1;
-}
-
 __device__ __forceinline__ long long table_find(const TableDev& t, uint64_t a, uint64_t b) {
   const uint64_t i = det_hash(a, b) & t.mask;
   uint64_t ka, kb;

@@ -799,7 +799,7 @@ constexpr int kShiftQ = 3;
 constexpr int kShiftRegRows = 36;
 constexpr int kShiftRegThreads = 160;
 
-__device__ inline bool shift_factor_reg(double* A, int lda, int n, double sigma, const EigVecs& V, double* Li) {
+__device__ bool shift_factor_reg(double* A, int lda, int n, double sigma, const EigVecs& V, double* Li) {
   const int t = threadIdx.x;
   const bool part = t < kShiftRegThreads;
   const int r = t >> 2, q = t & 3;
@@ -884,7 +884,7 @@ __device__ inline bool shift_factor_reg(double* A, int lda, int n, double sigma,
 // (n x lda shared doubles); (c) and (d) by one warp, up to kShiftQ rows per
 // lane, shuffle reductions and no block barrier, each refinement step
 // adding the residual's product with A (upper triangle and V.d).
-__device__ inline bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
+__device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs& V, double sigma, double* Li,
                                         double* Ci, int* steps, double* diff, SectionClock& clk) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ bool s_ok;
@@ -1162,7 +1162,7 @@ __device__ inline bool eig_lowest_shifted_warp(double* A, int lda, int n, const 
 constexpr int kBorderMaxK = 64;
 constexpr int kBorderIters = 64;
 
-__device__ inline bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, double* pack, int* iters,
+__device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVecs& V, double* pack, int* iters,
                                     double* resid, SectionClock& clk) {
   __shared__ int s_ok, s_it;
   __shared__ double s_rn;

@@ -79,7 +79,6 @@ GpuBatch::GpuBatch(const std::vector<const Fcidump*>& fcis, const SolverOptions&
       each[i].verbose = false;
       each[i].fill_gpu = false;      // the batch's columns fill the GPU together
       each[i].table_growth = false;  // the batch launches its instances' kernels itself
-      each[i].fused = false;
       each[i].table = pool_ + off;
       each[i].table_slots = caps[i];
       off += caps[i];

@@ -423,9 +423,6 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   groups_ = opt_.groups > 0 ? opt_.groups : groups_rule_;
   if (opt_.autotune && opt_.groups == 0 && groups_ > kMaxGroups) groups_ = kMaxGroups;
   list_ = column_list_size(opt_.m);
-  // Fused iteration: blocks of 512 threads, about three rounds each.
-  fused_groups_ = static_cast<int>(
-      std::max<long long>(1, std::min<long long>(kMaxGroups, (entries_ + 3 * 512 - 1) / (3 * 512))));
 
   // First table: large enough that two graphs' worth of iterations, each
   // inserting at most k whole columns, keep it below 3/4 full, and at least
@@ -476,8 +473,7 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
     off = align_up(off + n_wab * 8, 256);
     // The iteration's small buffers, in the same allocation after the tables.
     // Per-CTA partial lists for the largest CTA count the autotuner tries.
-    const size_t parts =
-        static_cast<size_t>(opt_.k) * std::max({groups_, fused_groups_, opt_.autotune ? kMaxGroups : 1});
+    const size_t parts = static_cast<size_t>(opt_.k) * std::max(groups_, opt_.autotune ? kMaxGroups : 1);
     const size_t mk = static_cast<size_t>(kMaxK) * opt_.m;
     size_t mo = off;
     auto carve = [&](size_t bytes) {
@@ -620,35 +616,6 @@ GpuSolver::GpuSolver(const Fcidump& fci, const SolverOptions& opt) : opt_(opt) {
   ll_.m = opt_.m;
   ll_.k_req = opt_.k;
   ll_.eig_method = opt_.eig_method;
-
-  // Fused iteration: one cooperative launch of one CTA per SM, when the
-  // device supports it, one CTA fits an SM and the records are small enough.
-  {
-    int coop = 0;
-    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device_) != cudaSuccess) coop = 0;
-    const size_t per_col = static_cast<size_t>(entries_);
-    const size_t n_rec = static_cast<size_t>(opt_.k) * per_col;
-    if (opt_.fused && coop && 32 * n_rec <= kFusedRecordBytes && fused_fits(fused_launch())) {
-      const size_t flags_bytes = align_up(sizeof(IterFlags), 256);
-      const size_t arr = align_up(n_rec * 8, 256);
-      try {
-        d_fused_ = device_alloc<unsigned char>(flags_bytes + 4 * arr, "fused iteration records");
-      } catch (...) {
-        release();
-        throw;
-      }
-      unsigned char* fb = static_cast<unsigned char*>(d_fused_);
-      d_flags_ = reinterpret_cast<IterFlags*>(fb);
-      rec_.v = reinterpret_cast<double*>(fb + flags_bytes);
-      rec_.code = reinterpret_cast<long long*>(fb + flags_bytes + arr);
-      rec_.a = reinterpret_cast<uint64_t*>(fb + flags_bytes + 2 * arr);
-      rec_.b = reinterpret_cast<uint64_t*>(fb + flags_bytes + 3 * arr);
-      rec_.per_col = static_cast<long long>(per_col);
-      fused_ctas_ = sms;
-      fused_ = true;
-    }
-    (void)cudaGetLastError();
-  }
   const auto t_sync = clock::now();
   const cudaError_t sync_err = cudaStreamSynchronize(stream_);
   setup_ms_[9] = ms_since(t_sync);
@@ -667,9 +634,6 @@ void GpuSolver::release() {
   cudaFree(d_tables_);
   if (own_table_) cudaFree(d_slots_);
   cudaFree(d_misc_);
-  cudaFree(d_fused_);
-  d_fused_ = nullptr;
-  d_flags_ = nullptr;
   d_misc_ = nullptr;
   d_sect_ = nullptr;
   d_part_key_ = nullptr;
@@ -709,7 +673,6 @@ void GpuSolver::reset() {
   h_state_.m = opt_.m;
   h_state_.occupancy_limit = static_cast<unsigned long long>(0.79 * static_cast<double>(max_size_));
   check(cudaMemcpyAsync(d_state_, &h_state_, sizeof(IterState), cudaMemcpyHostToDevice, stream_), "state upload");
-  if (fused_) check(cudaMemsetAsync(d_flags_, 0, sizeof(IterFlags), stream_), "memset");
   check(launch_init(ll_, ref_, ref_diag_, stream_), "init");
   check(launch_column(cl_, stream_), "column (init)");
   // The initial column inserts at most one column's entries.
@@ -719,51 +682,19 @@ void GpuSolver::reset() {
   occ_exact_iters_ = 0;
 }
 
-FusedLaunch GpuSolver::fused_launch() const {
-  FusedLaunch f;
-  f.lead = ll_;
-  f.col = cl_;
-  f.col.groups = fused_groups_;
-  f.flags = d_flags_;
-  f.rec = rec_;
-  return f;
-}
-
-cudaError_t GpuSolver::launch_one_iteration() {
-  if (fused_) return launch_fused(fused_launch(), fused_ctas_, stream_);
-  const cudaError_t e = launch_leader(ll_, stream_);
-  if (e != cudaSuccess) return e;
-  return launch_column(cl_, stream_);
-}
-
 void GpuSolver::build_graph() {
   const auto t0 = std::chrono::steady_clock::now();
   // Launch attributes are set outside the capture.
   check(prepare_leader(ll_), "leader attributes");
   cudaGraph_t g = nullptr;
   check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-  cudaError_t le = cudaSuccess;
-  for (long long i = 0; i < graph_iters_ && le == cudaSuccess; ++i) le = launch_one_iteration();
-  const cudaError_t ce = cudaStreamEndCapture(stream_, &g);
-  if (fused_ && (le != cudaSuccess || ce != cudaSuccess)) {
-    // A cooperative launch that cannot be captured: run chunks as direct launches.
-    if (g) cudaGraphDestroy(g);
-    (void)cudaGetLastError();
-    graph_failed_ = true;
-    setup_ms_[4] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    return;
+  for (long long i = 0; i < graph_iters_; ++i) {
+    launch_leader(ll_, stream_);
+    launch_column(cl_, stream_);
   }
-  check(le, "capture launch");
-  check(ce, "end capture");
-  const cudaError_t ie = cudaGraphInstantiate(&graph_, g, 0);
+  check(cudaStreamEndCapture(stream_, &g), "end capture");
+  check(cudaGraphInstantiate(&graph_, g, 0), "graph instantiate");
   cudaGraphDestroy(g);
-  if (fused_ && ie != cudaSuccess) {
-    graph_ = nullptr;
-    (void)cudaGetLastError();
-    graph_failed_ = true;
-  } else {
-    check(ie, "graph instantiate");
-  }
   setup_ms_[4] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -868,14 +799,15 @@ void GpuSolver::grow_to(size_t new_capacity) {
 }
 
 void GpuSolver::launch_chunk(long long n) {
-  if (n == graph_iters_ && !graph_failed_) {
+  if (n == graph_iters_) {
     if (!graph_) build_graph();
-    if (graph_) {
-      check(cudaGraphLaunch(graph_, stream_), "graph launch");
-      return;
-    }
+    check(cudaGraphLaunch(graph_, stream_), "graph launch");
+    return;
   }
-  for (long long i = 0; i < n; ++i) check(launch_one_iteration(), "iteration");
+  for (long long i = 0; i < n; ++i) {
+    check(launch_leader(ll_, stream_), "leader");
+    check(launch_column(cl_, stream_), "column");
+  }
 }
 
 namespace {
@@ -939,7 +871,7 @@ long long GpuSolver::autotune_groups(long long budget) {
 }
 
 void GpuSolver::run_iterations(long long n) {
-  if (opt_.autotune && !fused_ && !tuned_ && opt_.groups == 0) n -= autotune_groups(n);
+  if (opt_.autotune && !tuned_ && opt_.groups == 0) n -= autotune_groups(n);
   while (n > 0) {
     const long long c = std::min(n, graph_iters_);
     ensure_room(c);
@@ -962,16 +894,9 @@ void GpuSolver::run_iterations_timed(long long n, double* leader_ms, double* col
       ensure_room(c);
       for (long long i = i0; i < i0 + c; ++i) {
         check(cudaEventRecord(ev[3 * i], stream_), "cudaEventRecord");
-        if (fused_) {
-          // One kernel: its whole time counts as the leader's (the column
-          // work runs beside the leader and after it).
-          check(launch_fused(fused_launch(), fused_ctas_, stream_), "fused iteration");
-          check(cudaEventRecord(ev[3 * i + 1], stream_), "cudaEventRecord");
-        } else {
-          check(launch_leader(ll_, stream_), "leader");
-          check(cudaEventRecord(ev[3 * i + 1], stream_), "cudaEventRecord");
-          check(launch_column(cl_, stream_), "column");
-        }
+        check(launch_leader(ll_, stream_), "leader");
+        check(cudaEventRecord(ev[3 * i + 1], stream_), "cudaEventRecord");
+        check(launch_column(cl_, stream_), "column");
         check(cudaEventRecord(ev[3 * i + 2], stream_), "cudaEventRecord");
       }
       record_occupancy(c);
@@ -1009,8 +934,6 @@ void GpuSolver::read_state() {
                      "minimises ||H + x x^T||_F^2, which needs a negative ground-state energy; a positive core "
                      "energy in the FCIDUMP can make it positive).");
     if (err & kErrCandidates) throw McdError(MCD_ERR_NO_CANDIDATES, "The candidate list is empty.");
-    if (err & kErrWait)
-      throw McdError(MCD_ERR_CUDA, "a column CTA of the fused iteration kernel gave up waiting for its leader.");
     throw McdError(MCD_ERR_CUDA, "device error word " + std::to_string(err));
   }
 }

@@ -35,14 +35,8 @@ struct SolverOptions {
   // whole table is allocated at creation, as the reference reserves it.
   bool table_growth = true;
   // Subspace eigenproblem: 0 the full reduction every time; 1 shifted
-  // inverse iteration first, 2 the bordered fixed point first, with the
-  // reduction when the first method fails.
+  // inverse iteration first, with the reduction when it fails.
   int eig_method = 2;
-  // One cooperative launch per iteration (fused_iteration_kernel), whose
-  // column CTAs generate and probe the picked columns while the leader solves
-  // the subspace eigenproblem; used when the device allows it and the probe
-  // records fit kFusedRecordBytes.  false: the leader and column kernels.
-  bool fused = true;
   // Choose the CTAs per Hamiltonian column from timed trials (real
   // iterations of the solve) the first time enough iterations are run, and
   // remember the choice per (orbitals, electrons, k, m, SM count).
@@ -142,12 +136,6 @@ class GpuSolver {
   // 8 and 9 are parts of 2: the copy of the tables into pinned staging and
   // the constructor's final synchronisation with the stream.
   static constexpr int kSetupStages = 10;
-  // Largest probe-record buffer (32 bytes per column entry) the fused
-  // iteration is used with; beyond it the leader and column kernels run.
-  static constexpr size_t kFusedRecordBytes = static_cast<size_t>(256) << 20;
-  bool fused() const { return fused_; }
-  int fused_ctas() const { return fused_ctas_; }
-  int fused_groups() const { return fused_groups_; }
   const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }
@@ -178,8 +166,6 @@ class GpuSolver {
   size_t next_capacity(size_t c) const;     // the capacity after c
   void record_occupancy(long long iters);   // async occupancy read after a chunk of iters
   void launch_chunk(long long n);           // n <= graph_iters_ iterations, graph or direct
-  cudaError_t launch_one_iteration();       // leader + column kernels, or the fused kernel
-  FusedLaunch fused_launch() const;
   // The autotuner: trials of kTuneIters iterations per candidate CTA count,
   // the fastest column kernel kept; returns the iterations it ran.
   long long autotune_groups(long long budget);
@@ -220,15 +206,6 @@ class GpuSolver {
   void* d_misc_ = nullptr;  // unused: the buffers from d_state_ to d_done_ follow the tables in d_tables_
   Slot* d_slots_ = nullptr;
   IterState* d_state_ = nullptr;
-  // Fused iteration (opt_.fused): hand-over words and probe records in one
-  // allocation; CTAs per launch (one per SM) and column blocks per column.
-  bool fused_ = false;
-  void* d_fused_ = nullptr;
-  IterFlags* d_flags_ = nullptr;
-  EntryRecords rec_{};
-  int fused_ctas_ = 0;
-  int fused_groups_ = 0;
-  bool graph_failed_ = false;  // a capture of the iteration failed: chunks run as direct launches
   double* d_cand_score_ = nullptr;
   unsigned* d_cand_slot_ = nullptr;
   double* d_hsub_ = nullptr;

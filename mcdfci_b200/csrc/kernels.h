@@ -93,31 +93,6 @@ struct ColumnLaunch {
   int na, nb;             // electrons per spin (fixed by the starting determinant)
 };
 
-// Hand-over inside one launch of the fused iteration kernel (CTA 0 the
-// leader, the others the column work; a cooperative launch, so all are
-// resident at once).  Sequence numbers only grow: a launch's number is
-// seq + 1, read by every CTA at its start; seq itself is advanced by the last
-// CTA of the launch to finish, after every CTA has read it.
-struct IterFlags {
-  unsigned long long seq;    // fused launches completed since the reset
-  unsigned long long picks;  // = the launch's number once the picked determinants and k_cur are published
-  unsigned long long dx;     // = the launch's number once dx and the iteration's scalars are (k_cur 0: none)
-  unsigned done;             // CTAs of the current launch that have finished
-  unsigned pad;
-};
-
-// What the probe phase of the fused kernel found for each column entry (entry
-// e of column c at c * per_col + e), for its update phase.
-struct EntryRecords {
-  double* v;        // H value (the diagonal entry's is H_sub's, filled in by the update)
-  long long* code;  // >= 0: the slot holding the determinant; <= -2: absent, -2 - code the first
-                    // empty slot of its probe run; kRecSkip: nothing to do
-  uint64_t* a;      // the determinant's strings (for an insert)
-  uint64_t* b;
-  long long per_col;
-};
-constexpr long long kRecSkip = -1;
-
 struct LeaderLaunch {
   HamDev ham;
   TableDev tab;
@@ -205,24 +180,6 @@ int column_groups(int entries, int k, int resident);
 constexpr int kMaxGroups = 96;
 constexpr int kTuneIters = 16;
 cudaError_t launch_column(const ColumnLaunch& a, cudaStream_t s);
-
-// One iteration as one cooperative launch of `ctas` CTAs of 512 threads (at
-// most one per SM): CTA 0 runs the leader, and publishes the picked
-// determinants (IterFlags::picks) before its subspace eigenproblem and dx
-// after it (IterFlags::dx); the other CTAs run the column kernel's
-// generation and probes of the picked columns as soon as the picks are out,
-// record what they found (EntryRecords), and apply the z updates and keep the
-// candidates once dx is out.  col.groups counts blocks of 512 entries' threads
-// per column.  Every wait is bounded (kErrWait).
-struct FusedLaunch {
-  LeaderLaunch lead;
-  ColumnLaunch col;
-  IterFlags* flags;
-  EntryRecords rec;
-};
-cudaError_t launch_fused(const FusedLaunch& f, int ctas, cudaStream_t s);
-// Whether one CTA of the fused kernel fits on an SM (1) or not (0).
-int fused_fits(const FusedLaunch& f);
 cudaError_t launch_leader(const LeaderLaunch& a, cudaStream_t s);
 // Sets, on the current device, the launch attribute launch_leader needs for
 // a (its dynamic shared-memory limit); for use before a stream capture.

@@ -624,22 +624,7 @@ __device__ bool topk_radix(const unsigned* us, const double* sc, int n, int k, c
 }
 
 
-// Release and acquire of a hand-over word of IterFlags (gpu scope).
-__device__ __forceinline__ void flag_release(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long flag_acquire(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// flags (the fused iteration kernel only): the picked determinants, their
-// slots and k_cur go to the iteration state as soon as they are known and
-// flags->picks is set to `seqno`; flags->dx once the update is published (on
-// every path, k_cur = 0 when there is nothing for the columns to do).
-__device__ __forceinline__ void leader_body(const LeaderLaunch& L, IterFlags* flags = nullptr,
-                                            unsigned long long seqno = 0) {
+__device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(16) IterState sS;
   __shared__ int s_off[kMaxK + 1];
@@ -704,11 +689,6 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L, IterFlags* fl
       G->xz = sS.xz;
       G->pending = 0;
       G->k_cur = 0;
-      if (flags) {
-        __threadfence();
-        flag_release(&flags->picks, seqno);
-        flag_release(&flags->dx, seqno);
-      }
     }
     return;
   }
@@ -867,16 +847,6 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L, IterFlags* fl
     s_det[tid] = Det{a, b};
     s_x[tid] = load_relaxed(&sp->x);
     s_z[tid] = load_relaxed(&sp->z);
-    if (flags) {
-      G->det[tid] = s_det[tid];
-      G->slot[tid] = s_slot[tid];
-    }
-  }
-  if (flags) {
-    if (tid == 0) G->k_cur = k;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) flag_release(&flags->picks, seqno);
   }
   __syncthreads();
   clk.mark(5);
@@ -929,10 +899,6 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L, IterFlags* fl
       G->xz = sS.xz;
       G->pending = 0;
       G->k_cur = 0;
-      if (flags) {
-        __threadfence();
-        flag_release(&flags->dx, seqno);
-      }
     }
     return;
   }
@@ -992,11 +958,6 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L, IterFlags* fl
     G->slot[tid] = s_slot[tid];
     G->dx[tid] = s_dx[tid];
     G->hdiag[tid] = Hs[tid * k + tid];
-  }
-  if (flags) {
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) flag_release(&flags->dx, seqno);
   }
   __syncthreads();
   clk.mark(8);

@@ -73,7 +73,6 @@ enum : unsigned {
   kErrOverflow = 2u,   // occupancy above the reference's 0.79 * max_wavefunction_size
   kErrEig = 4u,        // subspace eigenproblem produced a non-finite or invalid update
   kErrCandidates = 8u, // no candidate determinant to pick
-  kErrWait = 16u,      // a CTA of the fused iteration kernel gave up waiting for the leader
 };
 
 // The open-addressing (x, z) table in HBM.

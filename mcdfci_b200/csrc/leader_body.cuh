@@ -1,6 +1,6 @@
 // Device code of the leader: the serial part of one mCDFCI iteration, run by
 // one CTA of 512 threads (leader_body), with its helpers; included by the
-// leader kernels and by the fused iteration kernel.
+// leader kernels (leader_kernel.cu).
 //
 //   finish iteration t-1   z[D_c] = new_z_c for the picked D_c (the exact
 //                          recompute that overwrites the accumulated z,

@@ -1189,13 +1189,19 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
       double off = 0.0;
       int c = 0;
       if (own[q])
-        for (int j = 0; j < k; ++j) {
-          const double v = row[j];
-          if (j != i && v != 0.0) {
-            off += fabs(v);
-            pv[i * lda + c] = v;
-            pc[i * (2 * lda + 1) + c] = j;
-            ++c;
+        for (int j0 = 0; j0 < k; j0 += 8) {
+          double v8[8];  // eight loads in flight before the dependent stores
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) v8[jj] = j0 + jj < k ? row[j0 + jj] : 0.0;
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int j = j0 + jj;
+            if (j != i && v8[jj] != 0.0) {
+              off += fabs(v8[jj]);
+              pv[i * lda + c] = v8[jj];
+              pc[i * (2 * lda + 1) + c] = j;
+              ++c;
+            }
           }
         }
       cnt[q] = c;

@@ -738,8 +738,18 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
       const int r0 = tid, r1 = kLT + tid;
       const unsigned s0 = r0 < R ? slot_of(r0) : kNoSlot;
       const unsigned s1 = r1 < R ? slot_of(r1) : kNoSlot;
-      const double g0 = r0 < R ? score_at(s0) : 0.0;
-      const double g1 = r1 < R ? score_at(s1) : 0.0;
+      // The candidates' (x, z) loads are issued here and consumed after the
+      // duplicate removal, which needs only the slots, so that their latency
+      // overlaps it.
+      double x0 = 0.0, z0 = 0.0, x1 = 0.0, z1 = 0.0;
+      if (r0 < R) {
+        x0 = load_relaxed(&T.slots[s0].x);
+        z0 = load_relaxed(&T.slots[s0].z);
+      }
+      if (r1 < R) {
+        x1 = load_relaxed(&T.slots[s1].x);
+        z1 = load_relaxed(&T.slots[s1].z);
+      }
       __syncthreads();
       int p0 = -1, p1 = -1, chunk = 0;
       bool keep = r0 < R && hash_keep(s0);
@@ -761,8 +771,12 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
         __syncthreads();
       }
       // The hash set (which sc overlays) is no longer read.
-      if (p0 >= 0) sc[p0] = g0;
-      if (p1 >= 0) sc[p1] = g1;
+      auto score_xz = [&](double x, double z) {
+        const double g = score_of(x, z, xss);
+        return (g >= 0.0) ? g : 0.0;  // as score_at
+      };
+      if (p0 >= 0) sc[p0] = score_xz(x0, z0);
+      if (p1 >= 0) sc[p1] = score_xz(x1, z1);
     } else {
       for (int r = tid; r < R; r += kLT) us[r] = slot_of(r);
       __syncthreads();

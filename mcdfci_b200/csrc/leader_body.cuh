@@ -127,13 +127,15 @@ __device__ double diagonal_warp(const HamDev& h, Det d, unsigned char* occ) {
     nocc += __popc(m);
   }
   __syncwarp();
+  // <i|h|i> over the occupied i and <ij||ij> over the occupied pairs i < j,
+  // the (i, j) terms spread over the lanes (independent loads).
   double v = 0.0;
-  for (int x = lane; x < nocc; x += 32) {
-    const int i = occ[x];
-    double t = h.hdiag[i];
-    const double* row = h.d2 + static_cast<size_t>(i) * h.nso;
-    for (int y = x + 1; y < nocc; ++y) t += row[occ[y]];
-    v += t;
+  for (int x = lane; x < nocc; x += 32) v += h.hdiag[occ[x]];
+  const int nn = nocc * nocc;
+#pragma unroll 4
+  for (int t = lane; t < nn; t += 32) {
+    const int x = t / nocc, y = t - x * nocc;
+    if (y > x) v += h.d2[static_cast<size_t>(occ[x]) * h.nso + occ[y]];
   }
   v = warp_sum(v);
   __syncwarp();

@@ -47,24 +47,11 @@ __device__ double single_value_det(const HamDev& h, int s, int p, int r, uint64_
   const double* st = h.st + base * h.nso;
   double v = h.sh[base];
   uint64_t u = a | b;
-  // Four orbitals' terms are loaded before they are added, then added in the
-  // order of the one-by-one sum (alpha before beta, ascending orbitals); an
-  // absent term is +0, which leaves the sum unchanged.
   while (u) {
-    double t[8];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      t[2 * j] = 0.0;
-      t[2 * j + 1] = 0.0;
-      if (u) {
-        const int q = __ffsll(static_cast<long long>(u)) - 1;
-        u &= u - 1;
-        if ((a >> q) & 1ull) t[2 * j] = st[2 * q];
-        if ((b >> q) & 1ull) t[2 * j + 1] = st[2 * q + 1];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v += t[j];
+    const int q = __ffsll(static_cast<long long>(u)) - 1;
+    u &= u - 1;
+    if ((a >> q) & 1ull) v += st[2 * q];
+    if ((b >> q) & 1ull) v += st[2 * q + 1];
   }
   return v;
 }

@@ -951,8 +951,9 @@ __device__ __forceinline__ void leader_body(const LeaderLaunch& L) {
     G->last_branch = er.branch;
     // Energy drop of this update, for the next one's shift: the current
     // energy xz/xx minus the eigenvalue (the energy after the update).
-    const double drop = dd_to_d(dd_div(sS.xz, sS.xx)) - er.lambda;
-    G->eig_drop = er.branch == 1 ? fmax(drop, 1e-300) : 0.0;
+    // (only the shifted solver, eig_method 1, uses it)
+    const double drop = L.eig_method == 1 ? dd_to_d(dd_div(sS.xz, sS.xx)) - er.lambda : 0.0;
+    G->eig_drop = er.branch == 1 && L.eig_method == 1 ? fmax(drop, 1e-300) : 0.0;
     G->max_abs_evec = er.max_evec;
     G->inv_steps_curr = er.shift_steps;
     G->inv_diff_curr = er.shift_diff;

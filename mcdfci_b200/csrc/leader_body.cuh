@@ -177,7 +177,10 @@ __host__ __device__ constexpr size_t eig_work_doubles(int k) {
 // (an upper bound of lambda_1: the current vector lies in the subspace, and
 // its Rayleigh quotient there is xz/xx) and the current vector as the start;
 // the reduction runs when that fails or its residual is not below 1e-11
-// (1 + |lambda|).
+// (1 + |lambda|).  method 2: the bordered fixed point (eig_lowest_bordered)
+// runs first for k <= kBorderMaxK, the reduction when it does not certify its
+// result or the residual check fails.  The first iteration's problem (branch
+// 2, no bordering row) always takes the reduction.
 __device__ EigResult eig_update(const double* H, int k, const double* x, const double* z, dd xx, dd xz,
                                 double* dx, double* work, SectionClock& clk, double drop, int method) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -282,9 +285,9 @@ __device__ EigResult eig_update(const double* H, int k, const double* x, const d
   clk.mark(9);
 
   double* Ae = branch == 1 ? A : A + lda + 1;
-  const double e_cur = dd_to_d(dd_div(xz, xx));
   bool shifted = false;
   if (branch == 1 && n <= kShiftMaxN && drop > 0.0) {
+    const double e_cur = dd_to_d(dd_div(xz, xx));
     const double delta = fmax(16.0 * drop, 1e-9 * (1.0 + fabs(e_cur)));
     for (int i = tid; i < n; i += blockDim.x) V.y[i] = i == 0 ? y1 : x[i - 1];
     __syncthreads();

@@ -33,6 +33,10 @@
 // The caller forms the Rayleigh quotient from the original matrix, the
 // quantity that the reference's refined step approximates
 // (rq = v'Bv + 2 dv'Bv, src/solver.h:516-521).
+// Two faster solvers that fall back to the reduction follow: 5, shifted
+// inverse iteration from a certified shift, and 6, the bordered fixed point
+// (the default), a one-warp iteration on the structure of the subspace matrix
+// whose result is certified as the lowest eigenpair by interlacing.
 #pragma once
 
 #include "device_common.cuh"

@@ -1142,9 +1142,7 @@ __device__ bool eig_lowest_shifted_warp(double* A, int lda, int n, const EigVecs
 //    lambda = a + b'y.  One warp iterates
 //        y <- -(b + E y) / (d - lambda),   lambda <- a + b'y,
 //    which contracts by about max_i sum_j |E_ij| / (d_i - lambda) per step, less
-//    than 1 whenever lambda < g, accelerated by Chebyshev weights from step 1
-//    on with that Gershgorin bound of the step's linear part as its spectral
-//    radius (the weights change only the path, not the fixed point) (C is strongly diagonal in a subspace of picked
+//    than 1 whenever lambda < g (C is strongly diagonal in a subspace of picked
 //    determinants, most of which are not connected by a single or double
 //    excitation).  The product E y of a step also gives the residual of the
 //    current iterate, r_i = (b + E y)_i + (d_i - lambda) y_i (row 0's residual
@@ -1177,7 +1175,7 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
   if (warp == 0) {
     double* ys = V.y + 1;  // y_j at ys[j]
     const double a = A[0];
-    double d[2], b[2], y[2], offs[2];
+    double d[2], b[2], y[2];
     bool own[2];
     int cnt[2];
     double gl = 1e300, nb = 0.0, babs = 0.0;
@@ -1211,7 +1209,6 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
           }
         }
       cnt[q] = c;
-      offs[q] = off;
       y[q] = 0.0;
       if (own[q]) {
         gl = fmin(gl, d[q] - off);
@@ -1240,13 +1237,7 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
     for (int q = 0; q < 2; ++q) rcp[q] = own[q] ? 1.0 / (d[q] - lam) : 0.0;
     // The tests compare squared residual norms |r|^2 / |v|^2 cross-multiplied,
     // so that no division or square root sits on a step's chain.
-    double rrp = 1e300, vvp = 1.0;    // |r|^2 and |v|^2 of the previous step
-    double rrpp = 1e300, vvpp = 1.0;  // and of the one before
-    // Chebyshev acceleration from step 1 on: rho bounds the spectral radius of
-    // the step's linear part (D - lambda)^-1 E by Gershgorin at that step's
-    // lambda, om the Chebyshev weight, yp the iterate before.
-    double yp[2] = {0.0, 0.0};
-    double rho2 = 0.0, om = 1.0;
+    double rrp = 1e300, vvp = 1.0;  // |r|^2 and |v|^2 of the previous step
     bool ok = false;
     int t = 0;
     for (; t < kBorderIters; ++t) {
@@ -1278,27 +1269,11 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
             else
               rcp[q] = 1.0 / x;
           }
-          yn[q] = own[q] ? -s[q] * rcp[q] : 0.0;  // the plain (Jacobi) step
+          yn[q] = own[q] ? -s[q] * rcp[q] : 0.0;
         } else {
           s[q] = 0.0;
           yn[q] = 0.0;
         }
-      }
-      if (t == 1) {
-        double r = 0.0;
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-          if (own[q]) r = fmax(r, offs[q] * fabs(rcp[q]));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(~0u, r, o));
-        r = fmin(r, 0.99);
-        rho2 = r * r;
-      }
-      if (t >= 1) {
-        // omega_1 = 1, omega_2 = 2 / (2 - rho^2), omega_j = 1 / (1 - rho^2 omega_{j-1} / 4)
-        om = t == 1 ? 1.0 : (t == 2 ? 2.0 / (2.0 - rho2) : 1.0 / (1.0 - 0.25 * rho2 * om));
-#pragma unroll
-        for (int q = 0; q < 2; ++q) yn[q] = fma(om, yn[q] - yp[q], yp[q]);
       }
       clk.mark(18);
       // Residual of (lambda_t, v_t), |y_t|^2 and b'y_{t+1}, in one reduction.
@@ -1328,18 +1303,14 @@ __device__ bool eig_lowest_bordered(const double* A, int lda, int n, const EigVe
         if (lane == 0) s_rn = rn;
         break;
       }
-      // not contracting (rn > 0.9 rn two steps back: the accelerated residual
-      // need not fall every step), or lambda not below g
-      if ((t >= 12 && rr * vvpp > 0.81 * rrpp * vv) || (t >= 4 && !(lam < gl))) break;
+      // not contracting (rn > 0.9 rn_prev), or lambda not below g
+      if ((t >= 8 && rr * vvp > 0.81 * rrp * vv) || (t >= 4 && !(lam < gl))) break;
       clk.mark(19);
-      rrpp = rrp;
-      vvpp = vvp;
       rrp = rr;
       vvp = vv;
       __syncwarp();  // every lane has read y_t
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        yp[q] = y[q];
         y[q] = yn[q];
         if (own[q]) ys[lane + 32 * q] = yn[q];
       }

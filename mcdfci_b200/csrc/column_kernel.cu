@@ -230,23 +230,40 @@ __device__ __forceinline__ bool above_threshold(dd scale, double dz, double zt) 
 
 // ---------------------------------------------------------------------------
 
-// Merges a descending list stored in global memory by another CTA (read
-// through L2, bypassing L1).
+// Reads a descending list stored in global memory by another CTA (through
+// L2, bypassing L1), reversed into ascending order for the bitonic merge.
 template <int R>
-__device__ __forceinline__ void toplist_merge_global(TopList<R>& L, const unsigned long long* ok,
-                                                     const unsigned* op) {
+__device__ __forceinline__ void toplist_load_global(TopList<R>& T, const unsigned long long* ok,
+                                                    const unsigned* op) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int i = (R - 1 - j) * 32 + (31 - lane);
-    const unsigned long long k2 = __ldcg(ok + i);
-    const unsigned p2 = __ldcg(op + i);
-    if (k2 > L.k[j]) {
-      L.k[j] = k2;
-      L.p[j] = p2;
+    T.k[j] = __ldcg(ok + i);
+    T.p[j] = __ldcg(op + i);
+  }
+}
+
+// Merge a list held in ascending order (as toplist_load_global leaves it)
+// into the descending list L.
+template <int R>
+__device__ __forceinline__ void toplist_merge_loaded(TopList<R>& L, const TopList<R>& T) {
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    if (T.k[j] > L.k[j]) {
+      L.k[j] = T.k[j];
+      L.p[j] = T.p[j];
     }
   }
   bitonic_merge_desc<R>(L);
+}
+
+template <int R>
+__device__ __forceinline__ void toplist_merge_global(TopList<R>& L, const unsigned long long* ok,
+                                                     const unsigned* op) {
+  TopList<R> T;
+  toplist_load_global<R>(T, ok, op);
+  toplist_merge_loaded<R>(L, T);
 }
 
 // One CTA's share of one column: CTA `blk` of the launch described by L
@@ -406,8 +423,22 @@ __device__ __forceinline__ void column_body(const ColumnLaunch& L, int blk) {
   TopList<R> U;
   toplist_clear<R>(U);
   const size_t base = static_cast<size_t>(col) * G;
-  for (int gg = warp; gg < G; gg += kW)
-    toplist_merge_global<R>(U, L.part_key + (base + gg) * M, L.part_slot + (base + gg) * M);
+  {
+    // A warp's first kPre lists are all requested before the first merge, so
+    // their L2 round trips overlap; the merge order stays w, w+kW, ...
+    constexpr int kPre = 3;
+    TopList<R> T[kPre];
+#pragma unroll
+    for (int t = 0; t < kPre; ++t) {
+      const int gg = warp + t * kW;
+      if (gg < G) toplist_load_global<R>(T[t], L.part_key + (base + gg) * M, L.part_slot + (base + gg) * M);
+    }
+#pragma unroll
+    for (int t = 0; t < kPre; ++t)
+      if (warp + t * kW < G) toplist_merge_loaded<R>(U, T[t]);
+    for (int gg = warp + kPre * kW; gg < G; gg += kW)
+      toplist_merge_global<R>(U, L.part_key + (base + gg) * M, L.part_slot + (base + gg) * M);
+  }
   toplist_cta_merge<R>(U, &s_key[0][0], &s_pay[0][0]);
   if (warp == 0) {
     int n = 0;

@@ -655,12 +655,18 @@ def b200_arm(args, rank, world, local_rank):
         ext = torch.cuda.ExternalStream(solver.stream)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
+        g0, st0 = solver.table_info()["growths"], solver.setup_times()
         ev0.record(ext)
         solver.run_iterations(args.steps)
         ev1.record(ext)
         ev1.synchronize()
         torch.cuda.synchronize()
         sampler.stop()
+        st1 = solver.setup_times()
+        growth_timed = {"growths": solver.table_info()["growths"] - g0,
+                        "ms": st1["growth"] - st0["growth"],
+                        "rehash_ms": st1["growth_rehash"] - st0["growth_rehash"],
+                        "slots_after": solver.table_info()["capacity"]}
         if dist:
             dist.barrier()
         r1 = solver.report()
@@ -762,6 +768,7 @@ def b200_arm(args, rank, world, local_rank):
                 "clocks": clocks,
                 "energy": r1["energy"],
                 "z_size": r1["z_size"],
+                "table_growth_timed": growth_timed,
                 "aged": aged,
                 "autotune": tuned,
                 "e2e_detail": e2e,
@@ -813,6 +820,9 @@ def e2e_run(mc, fc, args, local_rank):
         "solve_table_fill_ms": stages["table_fill"],
         "solve_graph_build_ms": stages["graph_build"],
         "solve_table_growth_ms": stages["growth"],
+        "solve_table_growth_alloc_ms": stages["growth_alloc"],
+        "solve_table_growth_rehash_ms": stages["growth_rehash"],
+        "solve_table_growth_free_ms": stages["growth_free"],
         "solve_report_readback_ms": stages["reports"],
         "table_slots": table["capacity"], "table_slots_max": table["max_capacity"],
         "table_growths": table["growths"],

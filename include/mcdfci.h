@@ -325,19 +325,30 @@ int mcd_eig_update_static(int32_t k, const double* hsub, const double* x, const 
 /* One compaction now (see mcd_options.compaction) with the given z_threshold
  * (>= the current one); *occupied receives the slots in use after it. */
 int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied);
+/* One table growth now, as the solver makes when the table fills: the next
+ * size (double, or the full one), rehashed by mode 0 (the solver's: a
+ * doubling moves runs of whole clusters through shared memory and writes
+ * every new slot), 1 (the doubling with every entry inserted by global
+ * compare-and-swap) or 2 (fill, then an atomic insert of every entry).
+ * *wrap_slots receives the length of the old table's cluster through its
+ * last and first slots (0 when either is empty, -1 when longer than 2^16).
+ * MCD_ERR_INVALID at the full size.  No counterpart in the reference (its
+ * table has a fixed size). */
+int mcd_debug_grow(mcd_solver* s, int32_t mode, int64_t* wrap_slots);
 /* WaveFunctionCuckoo::debug_calculate_xx_xz (src/wavefunction.h:640-651):
  * sum over the table of x^2 and x*z (double-double), and the slot count. */
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied);
 /* The hash table: slots now, slots at full size (max_memory), growths so far. */
 int mcd_debug_table_info(const mcd_solver* s, uint64_t* capacity, uint64_t* max_capacity, int32_t* growths);
 /* Host wall time of the solver's set-up stages in milliseconds, up to n
- * (<= 10) of them: 0 Hamiltonian tables (host, on a host thread during 7 and
+ * (<= 13) of them: 0 Hamiltonian tables (host, on a host thread during 7 and
  * 1), 1 device allocations at creation, 2 the wait for the host tables and
  * their upload, 3 table fill of the last reset (synchronised), 4 CUDA graph
  * builds, 5 table growths, 6 report read-backs, 7 device and stream set-up,
  * 8 and 9 parts of 2 (the copy into pinned staging, the final stream
- * synchronisation), summed since creation.  No counterpart in the
- * reference. */
+ * synchronisation), 10, 11 and 12 parts of 5 (the new table's allocation,
+ * its fill and the rehash into it, the release of the old table), summed
+ * since creation.  No counterpart in the reference. */
 int mcd_debug_setup_times(const mcd_solver* s, double* ms, int32_t n);
 /* The autotuner's record: the fixed rule's CTAs per column, the chosen
  * ones, and up to cap trials (CTAs per column, column-kernel microseconds

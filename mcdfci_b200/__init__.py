@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "mcd_rdm", "mcd_debug_wavefunction", "mcd_debug_compact", "mcd_checkpoint_save", "mcd_checkpoint_load",
     "mcd_debug_column_sections", "mcd_residual", "mcd_debug_slots", "mcd_debug_eig_shifted", "mcd_debug_eig_method",
     "mcd_debug_table_info", "mcd_debug_setup_times", "mcd_batch_residual", "mcd_debug_scatter_rate_mode",
-    "mcd_debug_autotune_info", "mcd_batch_table_sums",
+    "mcd_debug_autotune_info", "mcd_batch_table_sums", "mcd_debug_grow",
 )
 
 
@@ -148,6 +148,7 @@ def library() -> ctypes.CDLL:
                                        _dp, _dp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.mcd_rdm.argtypes = [vp, _dp, _dp]
     L.mcd_debug_compact.argtypes = [vp, ctypes.c_double, _u64p]
+    L.mcd_debug_grow.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
     L.mcd_debug_column_sections.argtypes = [vp, _u64p, ctypes.c_int32, ctypes.c_int32]
     L.mcd_checkpoint_save.argtypes = [vp, ctypes.c_char_p]
     L.mcd_checkpoint_load.argtypes = [vp, ctypes.c_char_p]
@@ -485,7 +486,7 @@ class CDFCI:
         return h.reshape(k, k)
 
     SETUP_STAGES = ("host_tables", "device_alloc", "upload", "table_fill", "graph_build", "growth", "reports",
-                    "device_setup", "upload_copy", "upload_sync")
+                    "device_setup", "upload_copy", "upload_sync", "growth_alloc", "growth_rehash", "growth_free")
 
     def autotune_info(self) -> dict:
         rule, chosen, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
@@ -495,6 +496,13 @@ class CDFCI:
                                                  ctypes.byref(n)))
         return {"rule": rule.value, "chosen": chosen.value,
                 "trials": [{"groups": g[i], "column_us": us[i]} for i in range(min(n.value, 16))]}
+
+    def grow(self, mode: int = 0) -> int:
+        """One table growth now (mcd_debug_grow); returns the length of the
+        old table's cluster through its last and first slots."""
+        w = ctypes.c_int64()
+        _check(library().mcd_debug_grow(self._h, int(mode), ctypes.byref(w)))
+        return w.value
 
     def table_info(self) -> dict:
         c, mc, g = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()

@@ -663,6 +663,16 @@ int mcd_debug_compact(mcd_solver* s, double z_threshold, uint64_t* occupied) {
   });
 }
 
+int mcd_debug_grow(mcd_solver* s, int32_t mode, int64_t* wrap_slots) {
+  return guarded([&] {
+    if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");
+    long long w = 0;
+    if (!s->impl->grow_now(mode, &w)) return fail(MCD_ERR_INVALID, "the table is at its full size.");
+    if (wrap_slots) *wrap_slots = w;
+    return MCD_OK;
+  });
+}
+
 int mcd_debug_table_sums(mcd_solver* s, double xx[2], double xz[2], uint64_t* occupied) {
   return guarded([&] {
     if (!s) return fail(MCD_ERR_INVALID, "solver is NULL.");

@@ -180,6 +180,174 @@ __global__ void rehash_kernel(const Slot* src, size_t n, TableDev t) {
   }
 }
 
+// Doubling rehash with no atomics on global memory for all but a few slots.
+// When a table of C slots doubles, an entry whose home is p = hash & (C-1)
+// gets the home p or p + C (bit C of its hash).  Take the old slots strictly
+// between two empty ones e0 < e1 (a run of whole clusters): every entry sits
+// at or after its home with no empty slot between, so its home is in
+// (e0, e1), and for each x there the entries with homes in [x, e1) filled old
+// slots in [x, e1), so there are at most e1 - x of them.  Linear probing then
+// places the run's lower entries within [e0, e1) and its upper entries within
+// [e0 + C, e1 + C), in any insertion order.  CTA b owns the run from the
+// first empty slot at or after b * kRehashChunk to the first at or after
+// (b + 1) * kRehashChunk, or to the table's last empty slot: it places the
+// entries in shared memory (a 32-bit compare-and-swap per probe) and writes
+// both new ranges whole, empty slots included, so the new table needs no
+// separate fill.  These runs tile [W, Z) (W the first empty slot, Z the last).
+// The cluster that wraps from slot C-1 to slot 0 belongs to the extra last
+// CTA: it empties [Z, C + W) and [Z + C, 2C) + [0, W), which by the same
+// count hold all that cluster's entries, and inserts them with the global
+// compare-and-swap.  A run longer than kRehashRange takes that global path
+// too, within its own ranges.  The entry count does not change.
+constexpr int kRehashChunk = 1024;
+constexpr int kRehashRange = 2048;
+constexpr int kRehashThreads = 256;
+
+__device__ __forceinline__ bool old_slot_empty(const Slot* src, long long i) {
+  const ulonglong2 k = __ldg(reinterpret_cast<const ulonglong2*>(src + i));
+  return k.x == kEmptyKey && k.y == kEmptyKey;
+}
+
+// First empty slot of src in [from, to), else `to`.  Whole warp.
+__device__ __forceinline__ long long warp_first_empty(const Slot* src, long long from, long long to) {
+  const int lane = threadIdx.x & 31;
+  for (long long base = from; base < to; base += 32) {
+    const long long i = base + lane;
+    const unsigned m = __ballot_sync(~0u, i < to && old_slot_empty(src, i));
+    if (m) return base + (__ffs(m) - 1);
+  }
+  return to;
+}
+
+// Last empty slot of src in [from, to), else -1.  Whole warp.
+__device__ __forceinline__ long long warp_last_empty(const Slot* src, long long from, long long to) {
+  const int lane = threadIdx.x & 31;
+  for (long long top = to; top > from; top -= 32) {
+    const long long i = top - 1 - lane;
+    const unsigned m = __ballot_sync(~0u, i >= from && old_slot_empty(src, i));
+    if (m) return top - __ffs(m);
+  }
+  return -1;
+}
+
+// Inserts an entry absent from t, probing at most `limit` slots from its
+// home; false when none of them was empty.
+__device__ __forceinline__ bool rehash_insert_global(const TableDev& t, const Slot& s, long long limit) {
+  uint64_t i = det_hash(s.a, s.b) & t.mask;
+  for (long long p = 0; p < limit; ++p) {
+    uint64_t ka, kb;
+    load_key(t.slots + i, ka, kb);
+    if (ka == kEmptyKey && kb == kEmptyKey) {
+      uint64_t oa, ob;
+      cas_key(t.slots + i, s.a, s.b, oa, ob);
+      if (oa == kEmptyKey && ob == kEmptyKey) {
+        t.slots[i].x = s.x;
+        t.slots[i].z = s.z;
+        return true;
+      }
+    }
+    i = (i + 1) & t.mask;
+  }
+  return false;
+}
+
+// src: the old table of C slots (a power of two, no reserved slot); t: the
+// new one of 2C slots, written whole.  Grid: C / kRehashChunk + 1 CTAs of
+// kRehashThreads.  force_global sends every run down the global path.
+__global__ void rehash_double_kernel(const Slot* __restrict__ src, long long C, TableDev t, int force_global) {
+  __shared__ int s_lo[kRehashRange], s_hi[kRehashRange];
+  __shared__ long long s_e[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const Slot empty{kEmptyKey, kEmptyKey, 0.0, 0.0};
+  Slot* dst = t.slots;
+  const long long nchunks = C / kRehashChunk;
+
+  if (blockIdx.x == nchunks) {
+    // The cluster through slot C-1 and slot 0.
+    if (warp == 0) {
+      const long long w = warp_first_empty(src, 0, C);
+      if (lane == 0) s_e[0] = w;
+    } else if (warp == 1) {
+      const long long z = warp_last_empty(src, 0, C);
+      if (lane == 0) s_e[1] = z;
+    }
+    __syncthreads();
+    const long long W = s_e[0], Z = s_e[1];
+    if (W >= C || Z < 0) {  // no empty slot: never, the occupancy limit is below 1
+      if (threadIdx.x == 0) atomicOr(t.err, kErrProbe);
+      return;
+    }
+    const long long n = C - Z + W;  // the length of each of the two regions
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+      dst[Z + i] = empty;
+      dst[(Z + C + i) & (2 * C - 1)] = empty;
+    }
+    __syncthreads();
+    for (long long i = 1 + threadIdx.x; i < n; i += blockDim.x) {
+      const Slot sl = src[(Z + i) & (C - 1)];
+      if (sl.a == kEmptyKey && sl.b == kEmptyKey) continue;
+      if (!rehash_insert_global(t, sl, n)) atomicOr(t.err, kErrProbe);
+    }
+    return;
+  }
+
+  const long long s = static_cast<long long>(blockIdx.x) * kRehashChunk;
+  if (warp == 0) {
+    const long long e0 = warp_first_empty(src, s, C);
+    if (lane == 0) s_e[0] = e0;
+  } else if (warp == 1) {
+    long long e1 = warp_first_empty(src, s + kRehashChunk, C);
+    if (e1 == C) e1 = warp_last_empty(src, s, s + kRehashChunk);
+    if (lane == 0) s_e[1] = e1;
+  }
+  __syncthreads();
+  const long long e0 = s_e[0], e1 = s_e[1];
+  // e0 == C: no empty slot from s on (inside the wrapping cluster);
+  // e1 == e0: no run starts in this chunk.
+  if (e0 >= C || e1 <= e0) return;
+  const long long L = e1 - e0;
+
+  if (L > kRehashRange || force_global) {
+    for (long long i = threadIdx.x; i < L; i += blockDim.x) {
+      dst[e0 + i] = empty;
+      dst[e0 + C + i] = empty;
+    }
+    __syncthreads();
+    for (long long i = 1 + threadIdx.x; i < L; i += blockDim.x) {
+      const Slot sl = src[e0 + i];
+      if (sl.a == kEmptyKey && sl.b == kEmptyKey) continue;
+      if (!rehash_insert_global(t, sl, L)) atomicOr(t.err, kErrProbe);
+    }
+    return;
+  }
+
+  const int n = static_cast<int>(L);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    s_lo[i] = -1;
+    s_hi[i] = -1;
+  }
+  __syncthreads();
+  for (int i = 1 + threadIdx.x; i < n; i += blockDim.x) {
+    const ulonglong2 k = __ldg(reinterpret_cast<const ulonglong2*>(src + e0 + i));
+    if (k.x == kEmptyKey && k.y == kEmptyKey) continue;
+    const uint64_t h = det_hash(k.x, k.y);
+    int* arr = (h & static_cast<uint64_t>(C)) ? s_hi : s_lo;
+    int p = static_cast<int>(static_cast<long long>(h & static_cast<uint64_t>(C - 1)) - e0);
+    if (static_cast<long long>(h & static_cast<uint64_t>(C - 1)) <= e0 || p > i) {
+      atomicOr(t.err, kErrProbe);  // a home outside its run: not a linear-probing table
+      continue;
+    }
+    while (p < n && atomicCAS(arr + p, -1, i) != -1) ++p;
+    if (p >= n) atomicOr(t.err, kErrProbe);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int jl = s_lo[i], jh = s_hi[i];
+    dst[e0 + i] = jl >= 0 ? src[e0 + jl] : empty;
+    dst[e0 + C + i] = jh >= 0 ? src[e0 + jh] : empty;
+  }
+}
+
 // Candidate lists: (col < k_cur, i < cand_n[col]).  save: the slots'
 // contents; restore: find or insert each saved determinant, its new slot.
 __global__ void compact_cand_save_kernel(const Slot* slots, const IterState* st, const unsigned* cand_slot, int m,
@@ -211,6 +379,14 @@ __global__ void compact_cand_restore_kernel(TableDev t, const IterState* st, con
 
 cudaError_t launch_rehash(const Slot* src, size_t n, const TableDev& t, cudaStream_t s) {
   rehash_kernel<<<148 * 8, 256, 0, s>>>(src, n, t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rehash_double(const Slot* src, size_t n, const TableDev& t, bool force_global, cudaStream_t s) {
+  if (n < static_cast<size_t>(kRehashChunk) || (n & (n - 1)) != 0 || t.mask != 2 * n - 1) return cudaErrorInvalidValue;
+  const size_t blocks = n / kRehashChunk + 1;
+  rehash_double_kernel<<<static_cast<unsigned>(blocks), kRehashThreads, 0, s>>>(src, static_cast<long long>(n), t,
+                                                                                force_global ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -745,9 +921,31 @@ void GpuSolver::ensure_room(long long upcoming) {
   if (cap != capacity_) grow_to(cap);
 }
 
-void GpuSolver::grow_to(size_t new_capacity) {
+bool GpuSolver::grow_now(int mode, long long* wrap) {
+  if (mode < 0 || mode > 2) throw McdError(MCD_ERR_INVALID, "growth mode must be 0, 1 or 2.");
+  if (capacity_ >= max_capacity_) return false;
+  read_state();
+  if (wrap) {
+    const size_t w = std::min<size_t>(capacity_, static_cast<size_t>(1) << 16);
+    std::vector<Slot> head(w), tail(w);
+    check(cudaMemcpy(head.data(), d_slots_, w * sizeof(Slot), cudaMemcpyDeviceToHost), "table read");
+    check(cudaMemcpy(tail.data(), d_slots_ + (capacity_ - w), w * sizeof(Slot), cudaMemcpyDeviceToHost), "table read");
+    auto empty = [](const Slot& x) { return x.a == kEmptyKey && x.b == kEmptyKey; };
+    long long first = -1, last = -1;
+    for (size_t i = 0; i < w && first < 0; ++i)
+      if (empty(head[i])) first = static_cast<long long>(i);
+    for (size_t i = w; i-- > 0 && last < 0;)
+      if (empty(tail[i])) last = static_cast<long long>(i);
+    *wrap = (first < 0 || last < 0) ? -1 : first + static_cast<long long>(w) - 1 - last;
+  }
+  grow_to(next_capacity(capacity_), mode);
+  return true;
+}
+
+void GpuSolver::grow_to(size_t new_capacity, int mode) {
   const auto t0 = std::chrono::steady_clock::now();
   read_state();  // applies the pending end of the iteration; nothing in flight
+  const auto t_alloc = std::chrono::steady_clock::now();
   const int m = opt_.m;
   Slot* fresh = nullptr;
   Slot* saved = nullptr;
@@ -759,17 +957,27 @@ void GpuSolver::grow_to(size_t new_capacity) {
     throw McdError(MCD_ERR_CUDA, std::string("the hash table could not grow to ") + std::to_string(new_capacity) +
                                      " slots (device memory taken since the solver was created?): " + e.what());
   }
+  const auto t1 = std::chrono::steady_clock::now();
   TableDev t = td_;
   t.slots = fresh;
   t.mask = new_capacity - 1;
   t.max_probe = static_cast<int>(std::min<size_t>(new_capacity, 1u << 14));
-  cudaError_t e = launch_table_fill(fresh, new_capacity, stream_);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_);
+  // A doubling (below 2^32 slots, where no slot is reserved) moves runs of
+  // clusters whole and writes every new slot; anything else is a fill and an
+  // insert of every entry, which recounts the occupancy.
+  const bool doubling = mode != 2 && new_capacity == 2 * capacity_ && new_capacity < (static_cast<size_t>(1) << 32);
+  cudaError_t e = cudaSuccess;
+  if (!doubling) {
+    e = launch_table_fill(fresh, new_capacity, stream_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_occ_, 0, sizeof(unsigned long long), stream_);
+  }
   if (e == cudaSuccess) {
     compact_cand_save_kernel<<<kMaxK, 128, 0, stream_>>>(d_slots_, d_state_, d_cand_slot_, m, saved);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = launch_rehash(d_slots_, capacity_, t, stream_);
+  if (e == cudaSuccess)
+    e = doubling ? launch_rehash_double(d_slots_, capacity_, t, mode == 1, stream_)
+                 : launch_rehash(d_slots_, capacity_, t, stream_);
   if (e == cudaSuccess) {
     compact_cand_restore_kernel<<<kMaxK, 128, 0, stream_>>>(t, d_state_, saved, d_cand_slot_, m);
     e = cudaGetLastError();
@@ -777,12 +985,17 @@ void GpuSolver::grow_to(size_t new_capacity) {
   unsigned long long occ = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&occ, d_occ_, sizeof(occ), cudaMemcpyDeviceToHost, stream_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  const auto t2 = std::chrono::steady_clock::now();
   cudaFree(saved);
   if (e != cudaSuccess) {
     cudaFree(fresh);
     check(e, "table growth");
   }
   cudaFree(d_slots_);
+  const auto t3 = std::chrono::steady_clock::now();
+  setup_ms_[10] += std::chrono::duration<double, std::milli>(t1 - t_alloc).count();
+  setup_ms_[11] += std::chrono::duration<double, std::milli>(t2 - t1).count();
+  setup_ms_[12] += std::chrono::duration<double, std::milli>(t3 - t2).count();
   d_slots_ = fresh;
   capacity_ = new_capacity;
   td_ = t;

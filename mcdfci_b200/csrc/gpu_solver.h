@@ -104,6 +104,10 @@ class GpuSolver {
   // Raise z_threshold to `z_threshold` and remove the entries with x = 0 and
   // |z scale| <= z_threshold, rebuilding the table; returns the occupied slots.
   unsigned long long compact(double z_threshold);
+  // Doubles the table now (grow_to's modes); *wrap receives the slots of
+  // the old table's cluster through its last and first slots (0 when either
+  // is empty; -1 when longer than 2^16).  False at the full size.
+  bool grow_now(int mode, long long* wrap);
   // Checkpoint of the wavefunction and the iteration state (binary file);
   // loading needs a solver for the same problem, k and m, and a table large
   // enough for the saved entries, and continues where the saved solve stopped.
@@ -134,8 +138,10 @@ class GpuSolver {
   // read-backs (finish, state copy, synchronisation), 7 device and stream
   // set-up (device, stream, attributes, free memory), summed since creation;
   // 8 and 9 are parts of 2: the copy of the tables into pinned staging and
-  // the constructor's final synchronisation with the stream.
-  static constexpr int kSetupStages = 10;
+  // the constructor's final synchronisation with the stream; 10, 11 and 12
+  // are parts of 5: the new table's allocation, its fill and the rehash into
+  // it (synchronised), and the release of the old table.
+  static constexpr int kSetupStages = 13;
   const double* setup_ms() const { return setup_ms_; }
   unsigned long long max_wavefunction_size() const { return max_size_; }
   int groups() const { return groups_; }
@@ -162,7 +168,11 @@ class GpuSolver {
   // whole column per coordinate, from the occupancy read (lagged by one
   // chunk) after earlier chunks; grows, synchronously, when it might not.
   void ensure_room(long long upcoming);
-  void grow_to(size_t new_capacity);        // rehash into a table of new_capacity slots
+  // Rehash into a table of new_capacity slots.  mode 0: a doubling moves runs
+  // of clusters (launch_rehash_double), other sizes fill and insert; 1: the
+  // doubling with every entry inserted by global compare-and-swap; 2: fill
+  // and insert whatever the size.
+  void grow_to(size_t new_capacity, int mode = 0);
   size_t next_capacity(size_t c) const;     // the capacity after c
   void record_occupancy(long long iters);   // async occupancy read after a chunk of iters
   void launch_chunk(long long n);           // n <= graph_iters_ iterations, graph or direct

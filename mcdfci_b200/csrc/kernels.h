@@ -193,6 +193,11 @@ cudaError_t launch_init(const LeaderLaunch& a, Det hf, double hf_diag, cudaStrea
 cudaError_t launch_finish(const LeaderLaunch& a, cudaStream_t s);
 // Every occupied slot of `src` (n slots) inserted into table t with its x and z.
 cudaError_t launch_rehash(const Slot* src, size_t n, const TableDev& t, cudaStream_t s);
+// The same for a table t of exactly 2n slots (n a power of two >= 1024, below
+// 2^32 in t), which it writes whole (no fill first) and whose occupancy
+// count it leaves as it is; force_global inserts every entry with the global
+// compare-and-swap instead of placing runs of clusters in shared memory.
+cudaError_t launch_rehash_double(const Slot* src, size_t n, const TableDev& t, bool force_global, cudaStream_t s);
 // Table initialisation (all slots empty) and whole-table sums.
 cudaError_t launch_table_fill(Slot* slots, size_t n, cudaStream_t s);
 cudaError_t launch_table_sums(const Slot* slots, size_t n, dd* partial, unsigned long long* count, int nblocks,

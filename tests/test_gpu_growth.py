@@ -94,3 +94,57 @@ def test_checkpoint_loads_into_a_smaller_first_table(synth_fcidumps, tmp_path):
     assert r_b["iteration"] == r_a["iteration"]
     assert abs(r_b["energy"] - r_a["energy"]) < 1e-9
     b.close()
+
+
+def _sorted_slots(s):
+    import numpy as np
+
+    a, b, x, z = s.slots()
+    o = np.lexsort((b, a))
+    return a[o], b[o], x[o], z[o]
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_doubling_rehash_keeps_every_entry(synth_fcidumps, mode):
+    """A doubling moves runs of whole clusters (mode 0: placed in shared
+    memory; mode 1: every entry by global compare-and-swap), and writes every
+    slot of the new table: the same determinants with the same x and z, the
+    same occupancy, and (k = 1) the same solve afterwards as the fill and
+    insert of mode 2."""
+    import numpy as np
+
+    path = synth_fcidumps["n16_5a5b"]
+    kw = dict(num_of_coordinate=1, estimate=16, max_memory=1.0, threshold=0.0, z_threshold=0.0)
+    solvers, wraps = {}, {}
+    for md in (mode, 2):
+        s = m.CDFCI(m.Fcidump(path), **kw)
+        s.reset()
+        s.run_iterations(1500)
+        before = _sorted_slots(s)
+        occ0 = s.report()["occupied"]
+        cap0 = s.table_info()["capacity"]
+        wraps[md] = [s.grow(md), s.grow(md)]
+        assert s.table_info()["capacity"] == 4 * cap0
+        after = _sorted_slots(s)
+        for u, v in zip(before, after):
+            assert np.array_equal(u, v)
+        r = s.report()
+        assert r["occupied"] == occ0 == len(before[0])
+        assert s.table_sums()["occupied"] == occ0
+        solvers[md] = s
+    # The occupied slots of linear probing do not depend on the insertion
+    # order, so both solvers saw the same clusters at the table ends.
+    assert wraps[mode] == wraps[2]
+    reps = {}
+    for md, s in solvers.items():
+        out = []
+        for _ in range(3):
+            s.run_iterations(200)
+            out.append(s.report())
+        reps[md] = out
+        s.close()
+    for a, b in zip(reps[mode], reps[2]):
+        assert a["iteration"] == b["iteration"]
+        assert abs(a["energy"] - b["energy"]) <= 1e-10 * abs(b["energy"])
+        for f in ("x_size", "z_size", "cols_size", "updates", "emitted_total", "updates_total", "occupied"):
+            assert a[f] == b[f], f

@@ -90,9 +90,10 @@ typedef struct mcd_options {
   int32_t compaction;
   /* 1 (default): the hash table starts at the size two 64-iteration chunks
    * (or num_iterations, when fewer) of worst-case inserts need (k whole
-   * columns per iteration, kept below 3/4 full) and doubles, rehashing into a new allocation between chunks, up to
-   * the table max_memory gives; occupancy limits and results are those of the
-   * full table.  0: the full table is allocated at creation, as the reference
+   * columns per iteration, kept below 3/4 full) and doubles, rehashing into
+   * a new allocation between chunks, when those could pass 3/4 or when its
+   * load passes 1/4 (shorter probes), up to the table max_memory gives;
+   * occupancy limits and results are those of the full table.  0: the full table is allocated at creation, as the reference
    * reserves its table.  A growth that finds the device memory taken by
    * others fails with MCD_ERR_CUDA.  No counterpart in the reference. */
   int32_t table_growth;

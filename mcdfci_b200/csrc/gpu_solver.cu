@@ -332,11 +332,12 @@ __global__ void rehash_double_kernel(const Slot* __restrict__ src, long long C, 
     if (k.x == kEmptyKey && k.y == kEmptyKey) continue;
     const uint64_t h = det_hash(k.x, k.y);
     int* arr = (h & static_cast<uint64_t>(C)) ? s_hi : s_lo;
-    int p = static_cast<int>(static_cast<long long>(h & static_cast<uint64_t>(C - 1)) - e0);
-    if (static_cast<long long>(h & static_cast<uint64_t>(C - 1)) <= e0 || p > i) {
+    const long long d = static_cast<long long>(h & static_cast<uint64_t>(C - 1)) - e0;
+    if (d <= 0 || d > i) {
       atomicOr(t.err, kErrProbe);  // a home outside its run: not a linear-probing table
       continue;
     }
+    int p = static_cast<int>(d);
     while (p < n && atomicCAS(arr + p, -1, i) != -1) ++p;
     if (p >= n) atomicOr(t.err, kErrProbe);
   }

@@ -165,8 +165,9 @@ class GpuSolver {
   void gather_slots(double zlim, std::vector<Slot>& out);  // occupied slots kept by zlim, in slot order
   // Table growth: before `upcoming` iterations are enqueued, make sure that
   // the table keeps its load below 3/4 even if every one of them inserts a
-  // whole column per coordinate, from the occupancy read (lagged by one
-  // chunk) after earlier chunks; grows, synchronously, when it might not.
+  // whole column per coordinate, and that the load reached is at most 1/4
+  // (shorter probes), from the occupancy read (lagged by one chunk) after
+  // earlier chunks; grows, synchronously, when either might not hold.
   void ensure_room(long long upcoming);
   // Rehash into a table of new_capacity slots.  mode 0: a doubling moves runs
   // of clusters (launch_rehash_double), other sizes fill and insert; 1: the

@@ -1,9 +1,9 @@
 """The hash table that grows on demand (mcd_options.table_growth, the default).
 
 The table starts at the size that two 64-iteration chunks of worst-case
-inserts need and doubles by rehashing as it fills, up to the table max_memory
-gives.  Growth changes where determinants sit, not what the iteration
-computes:
+inserts need and doubles by rehashing as it fills (when the worst case could
+pass 3/4, or the load passes 1/4), up to the table max_memory gives.  Growth
+changes where determinants sit, not what the iteration computes:
 
 - with k = 1 (one column per iteration, so no two adds race on a slot) a solve
   that grows reports the same energies, sizes and counters as one that holds
@@ -13,7 +13,10 @@ computes:
   equal the sums over the table
   (WaveFunctionCuckoo::debug_calculate_xx_xz, src/wavefunction.h:640-667);
 - a checkpoint with more entries than a fresh solver's first table loads into
-  it (the table grows first) and continues the solve.
+  it (the table grows first) and continues the solve;
+- a doubling by runs of clusters (rehash_double_kernel, in shared memory or by
+  global compare-and-swap) keeps every determinant with its x and z, and the
+  solve after it follows the fill-and-insert rehash's exactly (k = 1).
 """
 import os
 

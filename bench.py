@@ -21,10 +21,14 @@ eigenproblem, apply x += dx and z += H_col * dx in the hash wavefunction.
                its average device time, against the measured HBM copy peak
   cpu_baseline the reference cdfci_omp, compiled from its sources, on a
                bounded sample of the same workload on this host's cores
+  table_growth_timed
+               the table growths inside value's timed iterations (they count
+               in it): how many, their host time and its rehash part
   aged         value's timing repeated after --aged-iterations iterations in
                all, on the grown table (load factor stated)
   e2e_detail   the end-to-end run's stages: host tables, device allocation,
-               upload, table fill, graph builds, growths, report read-backs
+               upload, table fill, graph builds, growths (with their
+               allocation, rehash and frees), report read-backs
 
   batched      the 32-point dissociation curve (synthetic n16_5a5b points,
                k = m = 16, 1 GB table each): coordinate updates/s of all 32

@@ -66,7 +66,7 @@ def _last_empty(src, lo, hi):
     return -1
 
 
-def _rehash(src, C, force_global, rng):
+def _rehash(src, C, force_global, rng, planted=None):
     N = 2 * C
     dst = ["unwritten"] * N
     writes = [0] * N
@@ -91,6 +91,8 @@ def _rehash(src, C, force_global, rng):
     rng.shuffle(blocks)  # CTAs in any order: their regions are disjoint
     for b in blocks:
         if b == C // CHUNK:
+            if planted == "no_wrap":
+                continue
             W, Z = _first_empty(src, 0, C), _last_empty(src, 0, C)
             n = C - Z + W
             for i in range(n):
@@ -106,6 +108,8 @@ def _rehash(src, C, force_global, rng):
         e1 = _first_empty(src, s + CHUNK, C)
         if e1 == C:
             e1 = _last_empty(src, s, s + CHUNK)
+        if planted == "chunk_cut":  # runs cut at the chunk bounds, not at empty slots
+            e0, e1 = max(s - 1, 0), min(s + CHUNK - 1, C - 1)
         if e0 >= C or e1 <= e0:
             continue
         L = e1 - e0
@@ -164,3 +168,25 @@ def test_doubling_rehash_runs(load, force_global, wrap):
     assert sum(e is not None for e in dst) == len(keys)
     if wrap:
         assert src[0] is not None and src[C - 1] is not None
+
+
+@pytest.mark.parametrize("planted", ["chunk_cut", "no_wrap"])
+def test_planted_mistakes_are_caught(planted):
+    """The checks above catch a rehash that cuts runs at the chunk bounds
+    (entries whose home lies in the previous chunk) or leaves out the
+    wrapping cluster."""
+    C = 1 << 12
+    rng = random.Random(7)
+    src, keys = _old_table(C, 0.75, rng, True)
+    try:
+        dst, writes, errors = _rehash(src, C, False, rng, planted)
+    except AssertionError:
+        return  # a probe reached a slot that no CTA wrote
+    N = 2 * C
+    lost = 0
+    for k, h in keys.items():
+        i = h & (N - 1)
+        while dst[i] not in (None, "unwritten") and dst[i][0] != k:
+            i = (i + 1) & (N - 1)
+        lost += dst[i] in (None, "unwritten")
+    assert errors or lost or any(w != 1 for w in writes)
